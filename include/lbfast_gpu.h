@@ -1,0 +1,165 @@
+/*
+ * lbfast_gpu.h -- C ABI of the B200 implementation of the LBFAST time step.
+ *
+ * The reference drives its GPU kernels through the Fortran module
+ * lb_cuda_driver (lb_cuda_driver_module.f90), called by the integrator
+ * (integrator_module.f90:39-46) on device-resident tiled arrays that the
+ * Fortran side owns.  This header replaces that module with a flat C
+ * interface a Fortran driver binds through iso_c_binding (bind(C)), in the
+ * style of the reference's only existing C binding (nvml_wrapper.c:6-33,
+ * nvml_interface_module.f90:6-20): integer status returns, value arguments
+ * for scalars, plain pointers for arrays.  The library owns the device
+ * fields; the caller exchanges host arrays in Fortran order (i fastest).
+ *
+ * Every function returns LBF_OK (0) or a negative LBF_E* code; the message
+ * of the last failure on the calling thread is returned by lbf_last_error.
+ * No exception crosses this boundary.
+ */
+#ifndef LBFAST_GPU_H
+#define LBFAST_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBF_ABI_VERSION 1
+
+enum {
+    LBF_OK = 0,
+    LBF_E_ARG = -1,      /* invalid argument */
+    LBF_E_CUDA = -2,     /* CUDA runtime error */
+    LBF_E_NOMEM = -3,    /* device or host allocation failed */
+    LBF_E_STATE = -4,    /* call out of order (e.g. step before set_fields) */
+    LBF_E_UNSUPPORTED = -5,
+    LBF_E_IO = -6,       /* file could not be read or written */
+    LBF_E_NUMERIC = -7   /* non-finite value detected */
+};
+
+/* storage of the moment fields in HBM */
+enum { LBF_STORE_F32 = 0, LBF_STORE_F16 = 1, LBF_STORE_BF16 = 2, LBF_STORE_F64 = 3 };
+/* element type of host arrays */
+enum { LBF_F32 = 0, LBF_F64 = 1 };
+
+/*
+ * Run parameters.  Mirrors the reference's compile-time macros (defines.h:1-74:
+ * LATTICE, HIGHORDER, TWOCOMPONENT, DENSRATIO -> INTERFACE_INCOMP,
+ * INTERNAL_OBSTACLES) and the `simulation` / `fluid` namelists
+ * (LBFAST.f90:32-60).  Derived quantities (tau, omega, beta, kappa, sharp_c)
+ * are computed inside with the formulas of LBFAST.f90:212-219.
+ */
+typedef struct lbf_params {
+    int lx, ly, lz;          /* box (one GPU: nx = lx etc.) */
+    int pbc_x, pbc_y, pbc_z; /* 1 = periodic */
+    int lattice;             /* 19 or 27 */
+    int highorder;           /* HIGHORDER, LATTICE 27 only */
+    int twocomponent;        /* TWOCOMPONENT */
+    int densratio;           /* DENSRATIO (requires twocomponent) */
+    int obstacles;           /* INTERNAL_OBSTACLES */
+    int storage;             /* LBF_STORE_* */
+    double visc1, visc2;     /* kinematic viscosities */
+    double rho_r, rho_b;     /* densities of the phi=1 and phi=0 fluids */
+    double sigma, width;     /* surface tension, interface width */
+    double tau_diff;         /* phase-field diffusivity */
+    double fx, fy, fz;       /* body force */
+    double wettab_r;         /* contact angle in degrees (obstacles, two components) */
+    int printphi;            /* PRINTPHI: `rho` output holds phi */
+    int zseg;                /* planes per z segment of the kernel; 0 = automatic */
+} lbf_params;
+
+typedef struct lbf_handle lbf_handle;
+
+/* Library version string; never fails. */
+const char* lbf_version(void);
+
+/* Message of the last failed call on this thread (truncated to n bytes). */
+int lbf_last_error(char* buf, size_t n);
+
+/* Replaces setup_cuda + allocate_struct (lb_cuda_driver_module.f90:44-168,
+ * allocate_module.f90:10-71): validates the parameters and allocates the
+ * device state on the current device. */
+int lbf_create(const lbf_params* p, lbf_handle** out);
+
+/* Frees the device state (the reference frees at program end). */
+int lbf_destroy(lbf_handle* h);
+
+/* Optional CUDA stream (cudaStream_t) for all later work of this handle. */
+int lbf_set_stream(lbf_handle* h, void* cuda_stream);
+
+/* isfluid as produced by LBFAST.f90:258-325 (values 1, -1, 0; int8, lx*ly*lz,
+ * Fortran order).  Required when obstacles = 1; otherwise all nodes are fluid. */
+int lbf_set_isfluid(lbf_handle* h, const int8_t* isfluid);
+
+/* Initial state, replacing the host->device mirror of hfields_flip /
+ * phifields_flip after initial_conditions_all (init_conditions_module.f90:15-589).
+ * mom10: 10 consecutive fields (P,u,v,w,Pxx,Pyy,Pzz,Pxy,Pxz,Pyz), each lx*ly*lz
+ * in Fortran order; phi: lx*ly*lz (two components; may be NULL otherwise).
+ * Both time levels receive these values, as `hfields_flop=hfields_flip`
+ * (init_conditions_module.f90:584-587).  dtype: LBF_F32 or LBF_F64. */
+int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype);
+
+/* Advances nsteps time steps: the body of the integrator loop
+ * (integrator_module.f90:270-825).  The first call after lbf_set_fields also
+ * performs the integrator's pre-loop wetting (integrator_module.f90:186-190).
+ * Asynchronous with respect to the host; errors of earlier launches surface
+ * here or at the next synchronising call. */
+int lbf_step(lbf_handle* h, int nsteps);
+
+/* Waits for the handle's stream and reports any device-side failure. */
+int lbf_sync(lbf_handle* h);
+
+/* Number of steps done since lbf_set_fields. */
+int lbf_get_step(lbf_handle* h, long long* step);
+
+/* State a next step starts from: moments (10 x N), phi (N) and the velocity
+ * after the force half-step of the last step (3 x N, the u_old of the next
+ * DENSRATIO force).  Any pointer may be NULL.  dtype: LBF_F32 or LBF_F64. */
+int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype);
+
+/* copy_print (print_module.f90:638-776, stepskip = 1) of the last step:
+ * rho (phi with printphi, rho_phi for two components with density ratio,
+ * phi for two components without, P for one component), vel (3 x N,
+ * interleaved per node as the reference's velprint(1:3,i,j,k)), press (P).
+ * float32, Fortran order.  Any pointer may be NULL. */
+int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press);
+
+/* Global sums in FP64 over fluid nodes (|isfluid| = 1): sum of phi, of P
+ * (mass) and of u, v, w (momentum), computed on the device.
+ * Counterpart of the reference's phi_sum_count_kernel
+ * (lb_cuda_boundary_module.f90:461-515) and sum_world_float
+ * (mpi_module.f90:7491-7560) on one rank.  out[5] = {phi, P, u, v, w}. */
+int lbf_reduce(lbf_handle* h, double out[5]);
+
+/* ---- host-side set-up helpers (the driver's part of LBFAST.f90) ---- */
+
+/* LBFAST.f90:258-325: from raw isfluid (1 fluid / 0 solid, as read from
+ * isfluid.raw) build the marked array: walls at non-periodic faces when
+ * obstacles = 1, then fluid nodes with a non-fluid neighbour become -1. */
+int lbf_mark_isfluid(int lx, int ly, int lz, int pbc_x, int pbc_y, int pbc_z, int lattice, int obstacles,
+                     const int8_t* raw, int8_t* out);
+
+/* Solid-node phi seeding of init_conditions_module.f90:492-541 (in place). */
+int lbf_seed_solid_phi(int lx, int ly, int lz, int lattice, const int8_t* isfluid, double* phi);
+
+/* Taylor-Green initial moments (init_conditions_module.f90:298-314), double,
+ * mom10 as in lbf_set_fields. */
+int lbf_ic_taylor_green(int lx, int ly, int lz, double u0, double* mom10);
+
+/* Droplet at rest with the Laplace pressure inside (default DOBENCHMARK
+ * branch, init_conditions_module.f90:394-426): phi and mom10 on fluid nodes. */
+int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
+                   double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* mom10, double* phi);
+
+/* raw + XDMF writer of print_raw_sync (print_module.f90:2007-2180): writes
+ * <dir>/out_rho_NNNNNN.raw/.xdmf, out_vel_..., and out_press_... when press
+ * is not NULL. */
+int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                       const float* press);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBFAST_GPU_H */

@@ -1,0 +1,11 @@
+"""lbfast_b200 -- B200-native (sm_100a) implementation of the LBFAST time step.
+
+The numerics run in the CUDA library built in-tree (lbfast_b200/_lib); this
+package binds its C ABI (include/lbfast_gpu.h) and adds the host-side pieces
+of the LBFAST driver (namelist reader, set-up, output).
+"""
+from .capi import (LbfError, Params, Solver, ic_droplet, ic_taylor_green, load, mark_isfluid,  # noqa: F401
+                   seed_solid_phi, write_raw_xdmf)
+
+__all__ = ["LbfError", "Params", "Solver", "ic_droplet", "ic_taylor_green", "load", "mark_isfluid",
+           "seed_solid_phi", "write_raw_xdmf"]

@@ -1,0 +1,279 @@
+"""ctypes binding of the C ABI in include/lbfast_gpu.h.
+
+This is the Python-side stand-in for the Fortran ``bind(C)`` interface a
+reference driver would use: every call goes through the
+same exported C symbols.  The shared library is the in-tree build
+``lbfast_b200/_lib/liblbfast_b200.so``; there is no fallback -- if it is
+missing or fails to load, importing the solver raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "liblbfast_b200.so")
+
+LBF_OK = 0
+STORE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
+LBF_F32, LBF_F64 = 0, 1
+
+EXPORTED = (
+    "lbf_version", "lbf_last_error", "lbf_create", "lbf_destroy", "lbf_set_stream", "lbf_set_isfluid",
+    "lbf_set_fields", "lbf_step", "lbf_sync", "lbf_get_step", "lbf_get_fields", "lbf_get_print_fields",
+    "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
+    "lbf_write_raw_xdmf",
+)
+
+
+class LbfParams(C.Structure):
+    _fields_ = [
+        ("lx", C.c_int), ("ly", C.c_int), ("lz", C.c_int),
+        ("pbc_x", C.c_int), ("pbc_y", C.c_int), ("pbc_z", C.c_int),
+        ("lattice", C.c_int), ("highorder", C.c_int), ("twocomponent", C.c_int),
+        ("densratio", C.c_int), ("obstacles", C.c_int), ("storage", C.c_int),
+        ("visc1", C.c_double), ("visc2", C.c_double), ("rho_r", C.c_double), ("rho_b", C.c_double),
+        ("sigma", C.c_double), ("width", C.c_double), ("tau_diff", C.c_double),
+        ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
+        ("printphi", C.c_int), ("zseg", C.c_int),
+    ]
+
+
+class LbfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m lbfast_b200.build` (or __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp, dp, fp, i8p = C.c_void_p, P(C.c_double), P(C.c_float), P(C.c_int8)
+    lib.lbf_version.restype = C.c_char_p
+    lib.lbf_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    lib.lbf_create.argtypes = [P(LbfParams), P(vp)]
+    lib.lbf_destroy.argtypes = [vp]
+    lib.lbf_set_stream.argtypes = [vp, vp]
+    lib.lbf_set_isfluid.argtypes = [vp, i8p]
+    lib.lbf_set_fields.argtypes = [vp, vp, vp, C.c_int]
+    lib.lbf_step.argtypes = [vp, C.c_int]
+    lib.lbf_sync.argtypes = [vp]
+    lib.lbf_get_step.argtypes = [vp, P(C.c_longlong)]
+    lib.lbf_get_fields.argtypes = [vp, vp, vp, vp, C.c_int]
+    lib.lbf_get_print_fields.argtypes = [vp, fp, fp, fp]
+    lib.lbf_reduce.argtypes = [vp, dp]
+    lib.lbf_mark_isfluid.argtypes = [C.c_int] * 8 + [i8p, i8p]
+    lib.lbf_seed_solid_phi.argtypes = [C.c_int] * 4 + [i8p, dp]
+    lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
+    lib.lbf_ic_droplet.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
+    lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    for name in EXPORTED:
+        getattr(lib, name).restype = C.c_int if name != "lbf_version" else C.c_char_p
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load().lbf_last_error(buf, 1024)
+    return buf.value.decode()
+
+
+def check(rc: int) -> None:
+    if rc != LBF_OK:
+        raise LbfError(rc, last_error())
+
+
+def _ptr(a: np.ndarray | None, ctype=C.c_void_p):
+    if a is None:
+        return None
+    if ctype is C.c_void_p:
+        return C.c_void_p(a.ctypes.data)
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+@dataclass
+class Params:
+    """Run parameters (the reference's macros + `simulation`/`fluid` namelists)."""
+    lx: int
+    ly: int
+    lz: int
+    pbc_x: int = 1
+    pbc_y: int = 1
+    pbc_z: int = 1
+    lattice: int = 27
+    highorder: int = 0
+    twocomponent: int = 0
+    densratio: int = 0
+    obstacles: int = 0
+    storage: str = "f32"
+    visc1: float = 0.1
+    visc2: float = 0.1
+    rho_r: float = 1.0
+    rho_b: float = 1.0
+    sigma: float = 0.0
+    width: float = 4.0
+    tau_diff: float = 0.1
+    fx: float = 0.0
+    fy: float = 0.0
+    fz: float = 0.0
+    wettab_r: float = 90.0
+    printphi: int = 0
+    zseg: int = 0
+
+    def to_c(self) -> LbfParams:
+        p = LbfParams()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if f.name == "storage":
+                v = STORE[v]
+            setattr(p, f.name, v)
+        return p
+
+    def oracle_dict(self) -> dict:
+        d = {f.name: getattr(self, f.name) for f in fields(self)}
+        d["twocomp"] = d.pop("twocomponent")
+        return d
+
+    @property
+    def shape(self):
+        return (self.lz, self.ly, self.lx)
+
+
+class Solver:
+    """One box on the current CUDA device, driven through the C ABI.
+
+    Arrays are numpy (lz, ly, lx) views of Fortran-order fields; moments are
+    (10, lz, ly, lx) in the order P, u, v, w, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz.
+    """
+
+    def __init__(self, params: Params):
+        self.lib = load()
+        self.params = params
+        self.h = C.c_void_p()
+        check(self.lib.lbf_create(C.byref(params.to_c()), C.byref(self.h)))
+        self.shape = params.shape
+
+    def close(self) -> None:
+        if self.h:
+            check(self.lib.lbf_destroy(self.h))
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(self.lib.lbf_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_isfluid(self, isf: np.ndarray) -> None:
+        a = np.ascontiguousarray(isf, dtype=np.int8).reshape(self.shape)
+        check(self.lib.lbf_set_isfluid(self.h, _ptr(a, C.c_int8)))
+
+    def set_fields(self, mom10: np.ndarray, phi: np.ndarray | None = None) -> None:
+        dt = LBF_F64 if mom10.dtype == np.float64 else LBF_F32
+        npdt = np.float64 if dt == LBF_F64 else np.float32
+        m = np.ascontiguousarray(mom10, dtype=npdt).reshape((10,) + self.shape)
+        p = None if phi is None else np.ascontiguousarray(phi, dtype=npdt).reshape(self.shape)
+        check(self.lib.lbf_set_fields(self.h, _ptr(m), _ptr(p), dt))
+
+    def step(self, n: int = 1) -> None:
+        check(self.lib.lbf_step(self.h, int(n)))
+
+    def sync(self) -> None:
+        check(self.lib.lbf_sync(self.h))
+
+    @property
+    def nstep(self) -> int:
+        s = C.c_longlong()
+        check(self.lib.lbf_get_step(self.h, C.byref(s)))
+        return s.value
+
+    def get_fields(self, dtype=np.float64):
+        dt = LBF_F64 if dtype == np.float64 else LBF_F32
+        m = np.empty((10,) + self.shape, dtype=dtype)
+        p = np.empty(self.shape, dtype=dtype) if self.params.twocomponent else None
+        u = np.empty((3,) + self.shape, dtype=dtype)
+        check(self.lib.lbf_get_fields(self.h, _ptr(m), _ptr(p), _ptr(u), dt))
+        return m, p, u
+
+    def get_print(self):
+        """copy_print fields: rho (lz,ly,lx), vel (3,lz,ly,lx), press (lz,ly,lx), float32."""
+        rho = np.empty(self.shape, dtype=np.float32)
+        vel = np.empty(self.shape + (3,), dtype=np.float32)
+        press = np.empty(self.shape, dtype=np.float32)
+        check(self.lib.lbf_get_print_fields(self.h, _ptr(rho, C.c_float), _ptr(vel, C.c_float),
+                                            _ptr(press, C.c_float)))
+        return rho, np.moveaxis(vel, -1, 0), press
+
+    def reduce(self) -> np.ndarray:
+        out = np.zeros(5, dtype=np.float64)
+        check(self.lib.lbf_reduce(self.h, _ptr(out, C.c_double)))
+        return out
+
+
+# ---- host-side set-up helpers (C++ behind the C ABI) ----
+
+def mark_isfluid(raw: np.ndarray, pbc=(1, 1, 1), lattice: int = 27, obstacles: bool = True) -> np.ndarray:
+    lib = load()
+    lz, ly, lx = raw.shape
+    r = np.ascontiguousarray(raw, dtype=np.int8)
+    out = np.empty_like(r)
+    check(lib.lbf_mark_isfluid(lx, ly, lz, int(pbc[0]), int(pbc[1]), int(pbc[2]), int(lattice), int(obstacles),
+                               _ptr(r, C.c_int8), _ptr(out, C.c_int8)))
+    return out
+
+
+def seed_solid_phi(phi: np.ndarray, isf: np.ndarray, lattice: int = 27) -> np.ndarray:
+    lib = load()
+    lz, ly, lx = phi.shape
+    p = np.ascontiguousarray(phi, dtype=np.float64).copy()
+    i = np.ascontiguousarray(isf, dtype=np.int8)
+    check(lib.lbf_seed_solid_phi(lx, ly, lz, int(lattice), _ptr(i, C.c_int8), _ptr(p, C.c_double)))
+    return p
+
+
+def ic_taylor_green(lx: int, ly: int, lz: int, u0: float) -> np.ndarray:
+    m = np.empty((10, lz, ly, lx), dtype=np.float64)
+    check(load().lbf_ic_taylor_green(lx, ly, lz, float(u0), _ptr(m, C.c_double)))
+    return m
+
+
+def ic_droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio=True, isf=None):
+    m = np.empty((10, lz, ly, lx), dtype=np.float64)
+    phi = np.empty((lz, ly, lx), dtype=np.float64)
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    i = None if isf is None else np.ascontiguousarray(isf, dtype=np.int8)
+    check(load().lbf_ic_droplet(lx, ly, lz, _ptr(c, C.c_double), float(radius), float(width), float(sigma),
+                                float(rho_r), float(rho_b), int(densratio), _ptr(i, C.c_int8),
+                                _ptr(m, C.c_double), _ptr(phi, C.c_double)))
+    return m, phi
+
+
+def write_raw_xdmf(directory: str, iframe: int, rho, vel, press=None) -> None:
+    lz, ly, lx = rho.shape
+    r = np.ascontiguousarray(rho, dtype=np.float32)
+    v = np.ascontiguousarray(np.moveaxis(vel, 0, -1), dtype=np.float32)
+    p = None if press is None else np.ascontiguousarray(press, dtype=np.float32)
+    check(load().lbf_write_raw_xdmf(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float),
+                                    _ptr(v, C.c_float), _ptr(p, C.c_float)))

@@ -1,0 +1,593 @@
+// lbf_capi.cu -- implementation of include/lbfast_gpu.h: device state,
+// step orchestration and the host boundary.
+//
+// Step orchestration (integrator_module.f90:266-827 on one GPU): per time
+// step one launch of the fused kernel, preceded -- with obstacles and two
+// components -- by the wetting kernel.  The reference's per-launch
+// cudaDeviceSynchronize (lb_cuda_driver_module.f90:944-983) is dropped:
+// launches are stream-ordered and errors are checked at synchronising calls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lbfast_gpu.h"
+#include "lbf_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(LBF_E_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+// D3Q27 link table (vars_module.f90:319-338); D3Q19 = first 19 links
+const int EXh[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, -1, 1, 1, -1};
+const int EYh[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, -1, 1};
+const int EZh[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1};
+
+}  // namespace
+
+struct lbf_handle {
+    lbf_params p;
+    int nx = 0, ny = 0, nz = 0;
+    long long N = 0;
+    int storage = 0;
+    size_t esz = 4, psz = 4;
+    bool tc = false, dr = false, obs = false;
+    double omega = 0, beta = 0, kapp = 0, sharp_c = 0;
+    double scale[lbf::NSCALE_H];
+    void* mom[2] = {nullptr, nullptr};
+    void* uold[2] = {nullptr, nullptr};
+    void* phi[2] = {nullptr, nullptr};
+    int8_t* isf = nullptr;
+    bool isf_set = false;
+    int cur = 0;
+    long long step = 0;
+    bool fields_set = false, primed = false;
+    bool u_valid = false;  // uold[cur] holds the post-force velocity of the last step
+    // wetting
+    int nwet = 0;
+    long long* wet_s = nullptr;
+    int* wet_donor = nullptr;
+    int* wet_flag = nullptr;
+    double* wet_wn = nullptr;
+    int* wet_shift = nullptr;
+    void* wetW[2] = {nullptr, nullptr};
+    int wet_pending = -1;         // W buffer holding ghost values not yet written
+    int wet_pending_target = -1;  // phi buffer they belong to
+    double cot_theta = 0;
+    cudaStream_t stream = nullptr;
+    int* d_err = nullptr;
+    double* d_red = nullptr;
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    lbf::StepLauncher launcher = nullptr;
+    int zseg = 0;
+};
+
+namespace {
+
+int ensure_staging(lbf_handle* h, size_t bytes) {
+    if (h->staging_bytes >= bytes) return LBF_OK;
+    if (h->staging) cudaFree(h->staging);
+    h->staging = nullptr;
+    h->staging_bytes = 0;
+    if (cudaMalloc(&h->staging, bytes) != cudaSuccess)
+        return fail(LBF_E_NOMEM, "device staging allocation of %zu bytes failed", bytes);
+    h->staging_bytes = bytes;
+    return LBF_OK;
+}
+
+void free_all(lbf_handle* h) {
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(h->mom[b]);
+        cudaFree(h->uold[b]);
+        cudaFree(h->phi[b]);
+        cudaFree(h->wetW[b]);
+    }
+    cudaFree(h->isf);
+    cudaFree(h->wet_s);
+    cudaFree(h->wet_donor);
+    cudaFree(h->wet_flag);
+    cudaFree(h->wet_wn);
+    cudaFree(h->wet_shift);
+    cudaFree(h->d_err);
+    cudaFree(h->d_red);
+    cudaFree(h->staging);
+}
+
+// automatic z segment: enough CTAs for a few waves on 148 SMs, segments of at
+// least 8 planes so the pipeline fill (5 planes) stays a small overhead
+int auto_zseg(int nx, int ny, int nz) {
+    long long cols = (long long)((nx + 31) / 32) * ((ny + 7) / 8);
+    long long target = 148LL * 2 * 4;
+    int nseg = (int)std::max<long long>(1, (target + cols - 1) / cols);
+    int zseg = (nz + nseg - 1) / nseg;
+    zseg = std::max(zseg, std::min(nz, 8));
+    return zseg;
+}
+
+// Pre-loop wetting of integrator_module.f90:186-190 / one launch per step.
+int launch_wet(lbf_handle* h, int in_buf, int out_buf, bool prime) {
+    if (!(h->tc && h->obs) || h->nwet == 0) return LBF_OK;
+    lbf::WetArgs a;
+    a.n = h->nwet;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+    a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
+    a.s_idx = h->wet_s;
+    a.donor = h->wet_donor;
+    a.flag = h->wet_flag;
+    a.wn = h->wet_wn;
+    a.shift = h->wet_shift;
+    a.cot_theta = h->cot_theta;
+    a.pin = h->phi[in_buf];
+    a.prime = prime ? 1 : 0;
+    if (prime) {
+        // in place: the wetting only reads fluid donors and the node's own value
+        a.wout = h->wetW[0];
+        a.scatter_dst = nullptr;
+        a.scatter_src = nullptr;
+        CUDA_TRY(lbf::launch_wetting(h->storage, a, h->stream));
+        CUDA_TRY(lbf::launch_wet_apply(h->storage, h->nwet, h->wet_s, h->wetW[0], h->phi[in_buf], h->stream));
+        return LBF_OK;
+    }
+    int wbuf = h->wet_pending >= 0 ? 1 - h->wet_pending : 0;
+    // ghost values of the previous step belong to that step's input buffer,
+    // which is this step's output buffer and is not read during this step
+    if (h->wet_pending >= 0 && h->wet_pending_target == out_buf) {
+        a.scatter_dst = h->phi[out_buf];
+        a.scatter_src = h->wetW[h->wet_pending];
+    } else {
+        a.scatter_dst = nullptr;
+        a.scatter_src = nullptr;
+    }
+    a.wout = h->wetW[wbuf];
+    CUDA_TRY(lbf::launch_wetting(h->storage, a, h->stream));
+    h->wet_pending = wbuf;
+    h->wet_pending_target = in_buf;
+    return LBF_OK;
+}
+
+// write pending ghost values into their phi buffer (before phi is read out)
+int flush_wet(lbf_handle* h) {
+    if (h->wet_pending < 0) return LBF_OK;
+    CUDA_TRY(lbf::launch_wet_apply(h->storage, h->nwet, h->wet_s, h->wetW[h->wet_pending],
+                                   h->phi[h->wet_pending_target], h->stream));
+    return LBF_OK;
+}
+
+int prime(lbf_handle* h) {
+    int rc = launch_wet(h, h->cur, 1 - h->cur, true);
+    if (rc) return rc;
+    h->primed = true;
+    return LBF_OK;
+}
+
+// per-field storage scale for 16-bit storage: the largest magnitude maps into
+// [2^11, 2^12), leaving a factor 16 of headroom below the FP16 maximum
+double pick_scale(int storage, double maxabs, double fallback) {
+    if (storage != LBF_STORE_F16 && storage != LBF_STORE_BF16) return 1.0;
+    double m = maxabs > 0 ? maxabs : fallback;
+    int e = (int)std::floor(std::log2(2048.0 / m));
+    return std::ldexp(1.0, e);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lbf_version(void) { return "lbfast-b200 1.0 (sm_100a)"; }
+
+int lbf_last_error(char* buf, size_t n) {
+    if (!buf || n == 0) return LBF_E_ARG;
+    std::snprintf(buf, n, "%s", g_last_error.c_str());
+    return LBF_OK;
+}
+
+int lbf_create(const lbf_params* p, lbf_handle** out) {
+    if (!p || !out) return fail(LBF_E_ARG, "lbf_create: null argument");
+    *out = nullptr;
+    if (p->lx < 1 || p->ly < 1 || p->lz < 1) return fail(LBF_E_ARG, "box must be at least 1^3");
+    if ((long long)p->lx * p->ly * p->lz > (1LL << 31) - 1)
+        return fail(LBF_E_ARG, "box of %lld nodes exceeds 2^31-1", (long long)p->lx * p->ly * p->lz);
+    if (p->lattice != 19 && p->lattice != 27) return fail(LBF_E_UNSUPPORTED, "LATTICE %d not supported (19 or 27)", p->lattice);
+    if (p->highorder && p->lattice != 27) return fail(LBF_E_ARG, "HIGHORDER requires LATTICE 27");
+    if (p->densratio && !p->twocomponent) return fail(LBF_E_ARG, "DENSRATIO requires TWOCOMPONENT");
+    if (p->storage < 0 || p->storage > 3) return fail(LBF_E_ARG, "unknown storage %d", p->storage);
+    if (p->visc1 <= 0 || (p->twocomponent && p->visc2 <= 0)) return fail(LBF_E_ARG, "viscosities must be positive");
+    if (p->twocomponent && (p->width <= 0)) return fail(LBF_E_ARG, "interface width must be positive");
+    if (p->densratio && (p->rho_r <= 0 || p->rho_b <= 0)) return fail(LBF_E_ARG, "densities must be positive");
+    lbf_handle* h = new (std::nothrow) lbf_handle();
+    if (!h) return fail(LBF_E_NOMEM, "host allocation failed");
+    h->p = *p;
+    h->nx = p->lx; h->ny = p->ly; h->nz = p->lz;
+    h->N = (long long)p->lx * p->ly * p->lz;
+    h->storage = p->storage;
+    h->esz = lbf::storage_bytes(p->storage);
+    h->psz = lbf::phi_bytes(p->storage);
+    h->tc = p->twocomponent != 0;
+    h->dr = p->densratio != 0;
+    h->obs = p->obstacles != 0;
+    // LBFAST.f90:212-219
+    double tau1 = p->visc1 * 3.0 + 0.5;
+    h->omega = 1.0 / tau1;
+    if (h->tc) {
+        h->beta = 12.0 * p->sigma / p->width;
+        h->kapp = 1.5 * p->sigma * p->width;
+        h->sharp_c = 4.0 * p->tau_diff / p->width;
+    }
+    {
+        const double pi = 3.1415926535897932384626433832795028841971;
+        double th = (180.0 - p->wettab_r) * pi / 180.0;
+        double s = std::sin(th), c = std::cos(th);
+        h->cot_theta = std::fabs(s) < 1.0e-14 ? std::copysign(1.0e14, c) : c / s;
+    }
+    for (int i = 0; i < lbf::NSCALE_H; ++i) h->scale[i] = 1.0;
+    switch (p->storage) {
+        case LBF_STORE_F32: h->launcher = lbf::step_launcher_f32(p->lattice, p->highorder, p->twocomponent); break;
+        case LBF_STORE_F16: h->launcher = lbf::step_launcher_f16(p->lattice, p->highorder, p->twocomponent); break;
+        case LBF_STORE_BF16: h->launcher = lbf::step_launcher_bf16(p->lattice, p->highorder, p->twocomponent); break;
+        case LBF_STORE_F64: h->launcher = lbf::step_launcher_f64(p->lattice, p->highorder, p->twocomponent); break;
+    }
+    if (!h->launcher) {
+        delete h;
+        return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
+    }
+    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : auto_zseg(h->nx, h->ny, h->nz);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b) {
+        ok = ok && cudaMalloc(&h->mom[b], 10 * h->N * h->esz) == cudaSuccess;
+        ok = ok && cudaMalloc(&h->uold[b], 3 * h->N * h->esz) == cudaSuccess;
+        if (h->tc) ok = ok && cudaMalloc(&h->phi[b], h->N * h->psz) == cudaSuccess;
+    }
+    if (ok && h->obs) ok = cudaMalloc(&h->isf, h->N) == cudaSuccess;
+    if (ok) ok = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
+    if (ok) ok = cudaMalloc(&h->d_red, 5 * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        free_all(h);
+        size_t need = 2 * (13 * h->N * h->esz + (h->tc ? h->N * h->psz : 0)) + (h->obs ? h->N : 0);
+        delete h;
+        return fail(LBF_E_NOMEM, "device allocation of %.3f GB failed", need / 1e9);
+    }
+    cudaMemset(h->d_err, 0, sizeof(int));
+    if (h->obs) cudaMemset(h->isf, 1, h->N);
+    *out = h;
+    return LBF_OK;
+}
+
+int lbf_destroy(lbf_handle* h) {
+    if (!h) return fail(LBF_E_ARG, "lbf_destroy: null handle");
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return LBF_OK;
+}
+
+int lbf_set_stream(lbf_handle* h, void* s) {
+    if (!h) return fail(LBF_E_ARG, "null handle");
+    h->stream = static_cast<cudaStream_t>(s);
+    return LBF_OK;
+}
+
+int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
+    if (!h || !isf) return fail(LBF_E_ARG, "lbf_set_isfluid: null argument");
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    for (long long i = 0; i < h->N; ++i)
+        if (isf[i] != 0 && isf[i] != 1 && isf[i] != -1) return fail(LBF_E_ARG, "isfluid[%lld] = %d not in {1,-1,0}", i, isf[i]);
+    if (!h->obs) {
+        for (long long i = 0; i < h->N; ++i)
+            if (isf[i] != 1) return fail(LBF_E_ARG, "isfluid has non-fluid nodes but obstacles = 0");
+        return LBF_OK;
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->isf, isf, h->N, cudaMemcpyHostToDevice, h->stream));
+    h->isf_set = true;
+    if (!h->tc) return LBF_OK;
+    // wetting tables: PHI_int_boundary_kernel steps 1-2 (lb_cuda_boundary_module.f90:281-398),
+    // in double; they depend on isfluid only.
+    const int pb[3] = {h->p.pbc_x, h->p.pbc_y, h->p.pbc_z};
+    const int dims[3] = {nx, ny, nz};
+    const int nl = h->p.lattice == 27 ? 27 : 19;
+    auto isf_at = [&](int x, int y, int z) -> int {
+        int c[3] = {x, y, z};
+        for (int d = 0; d < 3; ++d) {
+            if (c[d] < 0 || c[d] >= dims[d]) {
+                if (!pb[d]) return 1;  // never-written halo keeps isfluid = 1
+                c[d] = (c[d] % dims[d] + dims[d]) % dims[d];
+            }
+        }
+        return isf[((long long)c[2] * ny + c[1]) * nx + c[0]];
+    };
+    std::vector<long long> vs;
+    std::vector<int> vd, vf, vsh;
+    std::vector<double> vwn;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                long long c = ((long long)k * ny + j) * nx + i;
+                if (isf[c] != 0) continue;
+                double wx = 0, wy = 0, wz = 0;
+                for (int l = 1; l < nl; ++l) {
+                    int d2 = EXh[l] * EXh[l] + EYh[l] * EYh[l] + EZh[l] * EZh[l];
+                    if (isf_at(i + EXh[l], j + EYh[l], k + EZh[l]) == 0) continue;
+                    double sc = d2 == 1 ? 1.0 : d2 == 2 ? 0.5 : 1.0 / 3.0;
+                    wx += sc * -EXh[l];
+                    wy += sc * -EYh[l];
+                    wz += sc * -EZh[l];
+                }
+                double wn = std::sqrt(wx * wx + wy * wy + wz * wz);
+                if (wn < 1.0e-14) continue;
+                wx /= wn; wy /= wn; wz /= wn;
+                double best = -1.0e30;
+                int bl = -1;
+                for (int l = 1; l < nl; ++l) {
+                    int d2 = EXh[l] * EXh[l] + EYh[l] * EYh[l] + EZh[l] * EZh[l];
+                    int f = isf_at(i + EXh[l], j + EYh[l], k + EZh[l]);
+                    if (f != 1 && f != -1) continue;
+                    double sc = d2 == 1 ? 1.0 : d2 == 2 ? 0.70710678118654752440 : 0.57735026918962576450;
+                    double score = (-EXh[l] * wx + -EYh[l] * wy + -EZh[l] * wz) * sc;
+                    if (score > best) { best = score; bl = l; }
+                }
+                if (bl < 0) continue;
+                int dc[3] = {i + EXh[bl], j + EYh[bl], k + EZh[bl]};
+                // the reference skips a donor on the low halo layer (local index 0)
+                if (dc[0] == -1 || dc[1] == -1 || dc[2] == -1) continue;
+                int flag = lbf::WET_NORMAL;
+                for (int d = 0; d < 3; ++d) {
+                    if (dc[d] >= dims[d]) {
+                        if (!pb[d]) flag = lbf::WET_OUTSIDE;
+                        else if (flag == lbf::WET_NORMAL) flag = lbf::WET_HIGHWRAP;
+                        dc[d] -= dims[d];
+                    }
+                }
+                if (flag == lbf::WET_OUTSIDE) dc[0] = dc[1] = dc[2] = 0;
+                vs.push_back(c);
+                vd.insert(vd.end(), {dc[0], dc[1], dc[2]});
+                vf.push_back(flag);
+                vwn.insert(vwn.end(), {wx, wy, wz});
+                vsh.insert(vsh.end(), {-EXh[bl], -EYh[bl], -EZh[bl]});
+            }
+    cudaFree(h->wet_s); cudaFree(h->wet_donor); cudaFree(h->wet_flag); cudaFree(h->wet_wn); cudaFree(h->wet_shift);
+    cudaFree(h->wetW[0]); cudaFree(h->wetW[1]);
+    h->wet_s = nullptr; h->wet_donor = nullptr; h->wet_flag = nullptr; h->wet_wn = nullptr; h->wet_shift = nullptr;
+    h->wetW[0] = h->wetW[1] = nullptr;
+    h->nwet = (int)vs.size();
+    h->wet_pending = -1;
+    if (h->nwet == 0) return LBF_OK;
+    CUDA_TRY(cudaMalloc(&h->wet_s, vs.size() * sizeof(long long)));
+    CUDA_TRY(cudaMalloc(&h->wet_donor, vd.size() * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&h->wet_flag, vf.size() * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&h->wet_wn, vwn.size() * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&h->wet_shift, vsh.size() * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&h->wetW[0], h->nwet * h->psz));
+    CUDA_TRY(cudaMalloc(&h->wetW[1], h->nwet * h->psz));
+    CUDA_TRY(cudaMemcpy(h->wet_s, vs.data(), vs.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->wet_donor, vd.data(), vd.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->wet_flag, vf.data(), vf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->wet_wn, vwn.data(), vwn.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->wet_shift, vsh.data(), vsh.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return LBF_OK;
+}
+
+int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype) {
+    if (!h || !mom10) return fail(LBF_E_ARG, "lbf_set_fields: null argument");
+    if (dtype != LBF_F32 && dtype != LBF_F64) return fail(LBF_E_ARG, "dtype must be LBF_F32 or LBF_F64");
+    if (h->tc && !phi) return fail(LBF_E_ARG, "two-component run needs phi");
+    if (h->obs && !h->isf_set) return fail(LBF_E_STATE, "obstacles: call lbf_set_isfluid before lbf_set_fields");
+    const size_t hb = dtype == LBF_F64 ? 8 : 4;
+    const long long N = h->N;
+    // per-field scales for 16-bit storage, from the data
+    if (h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16) {
+        const double fallback[10] = {1e-2, 1e-2, 1e-2, 1e-2, 1e-4, 1e-4, 1e-4, 1e-4, 1e-4, 1e-4};
+        for (int f = 0; f < 10; ++f) {
+            double m = 0;
+            for (long long i = 0; i < N; ++i) {
+                double v = dtype == LBF_F64 ? static_cast<const double*>(mom10)[f * N + i]
+                                            : static_cast<const float*>(mom10)[f * N + i];
+                if (std::isfinite(v)) m = std::max(m, std::fabs(v));
+            }
+            h->scale[f] = pick_scale(h->storage, m, fallback[f]);
+        }
+        for (int f = 0; f < 3; ++f) h->scale[lbf::NSCALE_H - 4 + f] = h->scale[1 + f];
+    }
+    int rc = ensure_staging(h, N * hb);
+    if (rc) return rc;
+    for (int f = 0; f < 10; ++f) {
+        const char* src = static_cast<const char*>(mom10) + f * N * hb;
+        CUDA_TRY(cudaMemcpyAsync(h->staging, src, N * hb, cudaMemcpyHostToDevice, h->stream));
+        for (int b = 0; b < 2; ++b) {
+            char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
+            CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, dst, N, h->scale[f], h->stream));
+            if (f >= 1 && f <= 3) {  // u_old of the first step = initial velocity (B := A)
+                char* udst = static_cast<char*>(h->uold[b]) + (f - 1) * N * h->esz;
+                CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, udst, N,
+                                                h->scale[lbf::NSCALE_H - 4 + f - 1], h->stream));
+            }
+        }
+    }
+    if (h->tc) {
+        CUDA_TRY(cudaMemcpyAsync(h->staging, phi, N * hb, cudaMemcpyHostToDevice, h->stream));
+        for (int b = 0; b < 2; ++b)
+            CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, dtype, h->phi[b], N, 1.0, h->stream));
+    }
+    h->cur = 0;
+    h->step = 0;
+    h->fields_set = true;
+    h->primed = false;
+    h->u_valid = false;
+    h->wet_pending = -1;
+    // the staging copies above are asynchronous with respect to the caller's
+    // host buffers: complete them before returning
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return LBF_OK;
+}
+
+int lbf_step(lbf_handle* h, int nsteps) {
+    if (!h) return fail(LBF_E_ARG, "lbf_step: null handle");
+    if (nsteps < 0) return fail(LBF_E_ARG, "nsteps < 0");
+    if (!h->fields_set) return fail(LBF_E_STATE, "lbf_step before lbf_set_fields");
+    if (!h->primed) {
+        int rc = prime(h);
+        if (rc) return rc;
+    }
+    lbf::StepArgs a;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+    a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
+    a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg;
+    a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
+    a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
+    a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;
+    a.fx = h->p.fx; a.fy = h->p.fy; a.fz = h->p.fz;
+    for (int i = 0; i < lbf::NSCALE_H; ++i) a.scale[i] = h->scale[i];
+    a.isf = h->obs ? h->isf : nullptr;
+    a.err = h->d_err;
+    for (int s = 0; s < nsteps; ++s) {
+        const int in = h->cur, out = 1 - h->cur;
+        int rc = launch_wet(h, in, out, false);
+        if (rc) return rc;
+        a.min = h->mom[in];
+        a.mout = h->mom[out];
+        a.uin = h->uold[in];
+        a.uout = h->uold[out];
+        a.pin = h->phi[in];
+        a.pout = h->phi[out];
+        a.write_u = (h->dr || s == nsteps - 1) ? 1 : 0;
+        cudaError_t e = h->launcher(a, h->stream);
+        if (e != cudaSuccess) return fail(LBF_E_CUDA, "step kernel launch: %s", cudaGetErrorString(e));
+        h->cur = out;
+        h->step++;
+        h->u_valid = a.write_u != 0;
+    }
+    return LBF_OK;
+}
+
+int lbf_sync(lbf_handle* h) {
+    if (!h) return fail(LBF_E_ARG, "lbf_sync: null handle");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CUDA_TRY(cudaGetLastError());
+    return LBF_OK;
+}
+
+int lbf_get_step(lbf_handle* h, long long* step) {
+    if (!h || !step) return fail(LBF_E_ARG, "lbf_get_step: null argument");
+    *step = h->step;
+    return LBF_OK;
+}
+
+int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype) {
+    if (!h) return fail(LBF_E_ARG, "lbf_get_fields: null handle");
+    if (dtype != LBF_F32 && dtype != LBF_F64) return fail(LBF_E_ARG, "dtype must be LBF_F32 or LBF_F64");
+    if (!h->fields_set) return fail(LBF_E_STATE, "lbf_get_fields before lbf_set_fields");
+    if (!h->primed) {
+        int rc = prime(h);
+        if (rc) return rc;
+    }
+    const size_t hb = dtype == LBF_F64 ? 8 : 4;
+    const long long N = h->N;
+    int rc = ensure_staging(h, N * hb);
+    if (rc) return rc;
+    auto out_field = [&](const void* src, bool is_phi, double inv, void* dst) -> int {
+        CUDA_TRY(lbf::launch_convert_out(h->storage, is_phi, src, h->staging, dtype, N, inv, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(dst, h->staging, N * hb, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return LBF_OK;
+    };
+    if (mom10)
+        for (int f = 0; f < 10; ++f) {
+            rc = out_field(static_cast<const char*>(h->mom[h->cur]) + f * N * h->esz, false, 1.0 / h->scale[f],
+                           static_cast<char*>(mom10) + f * N * hb);
+            if (rc) return rc;
+        }
+    if (phi && h->tc) {
+        rc = out_field(h->phi[h->cur], true, 1.0, phi);
+        if (rc) return rc;
+    }
+    if (uold) {
+        for (int f = 0; f < 3; ++f) {
+            const void* src = (h->u_valid || h->step == 0)
+                                  ? static_cast<const char*>(h->uold[h->cur]) + f * N * h->esz
+                                  : static_cast<const char*>(h->mom[h->cur]) + (1 + f) * N * h->esz;
+            double sc = (h->u_valid || h->step == 0) ? h->scale[lbf::NSCALE_H - 4 + f] : h->scale[1 + f];
+            rc = out_field(src, false, 1.0 / sc, static_cast<char*>(uold) + f * N * hb);
+            if (rc) return rc;
+        }
+    }
+    return LBF_OK;
+}
+
+int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press) {
+    if (!h) return fail(LBF_E_ARG, "lbf_get_print_fields: null handle");
+    if (!h->fields_set) return fail(LBF_E_STATE, "lbf_get_print_fields before lbf_set_fields");
+    if (!h->primed) {
+        int rc = prime(h);
+        if (rc) return rc;
+    }
+    int rc = flush_wet(h);
+    if (rc) return rc;
+    const long long N = h->N;
+    rc = ensure_staging(h, 5 * N * sizeof(float));
+    if (rc) return rc;
+    // the copy_print of step n reads the input buffer of step n after the force
+    // half-step: P of that buffer, the post-force velocity, phi after wetting
+    const int src = h->step == 0 ? h->cur : 1 - h->cur;
+    lbf::PrintArgs a;
+    a.N = N;
+    a.mode = !h->tc ? 0 : ((h->p.printphi || !h->dr) ? 1 : 2);
+    a.rho_r = h->p.rho_r;
+    a.rho_b = h->p.rho_b;
+    a.P = h->mom[src];
+    a.sP = 1.0 / h->scale[0];
+    if (h->step == 0) {
+        a.vel = static_cast<const char*>(h->mom[h->cur]) + 1 * N * h->esz;
+        for (int f = 0; f < 3; ++f) a.su[f] = 1.0 / h->scale[1 + f];
+    } else {
+        if (!h->u_valid) return fail(LBF_E_STATE, "velocity of the last step was not kept");
+        a.vel = h->uold[h->cur];
+        for (int f = 0; f < 3; ++f) a.su[f] = 1.0 / h->scale[lbf::NSCALE_H - 4 + f];
+    }
+    a.phi = h->tc ? h->phi[src] : nullptr;
+    float* d = static_cast<float*>(h->staging);
+    a.rho = rho ? d : nullptr;
+    a.vel_out = vel ? d + N : nullptr;
+    a.press = press ? d + 4 * N : nullptr;
+    CUDA_TRY(lbf::launch_print(h->storage, a, h->stream));
+    if (rho) CUDA_TRY(cudaMemcpyAsync(rho, d, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (vel) CUDA_TRY(cudaMemcpyAsync(vel, d + N, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (press) CUDA_TRY(cudaMemcpyAsync(press, d + 4 * N, N * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return LBF_OK;
+}
+
+int lbf_reduce(lbf_handle* h, double out[5]) {
+    if (!h || !out) return fail(LBF_E_ARG, "lbf_reduce: null argument");
+    if (!h->fields_set) return fail(LBF_E_STATE, "lbf_reduce before lbf_set_fields");
+    double inv[4];
+    for (int f = 0; f < 4; ++f) inv[f] = 1.0 / h->scale[f];
+    CUDA_TRY(lbf::launch_reduce(h->storage, h->N, h->mom[h->cur], h->tc ? h->phi[h->cur] : nullptr,
+                                h->obs ? h->isf : nullptr, inv, h->d_red, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(out, h->d_red, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return LBF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// lbf_internal.h -- declarations shared by the translation units of the
+// library (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace lbf {
+
+constexpr int NSCALE_H = 14;
+
+// Storage-agnostic arguments of one fused step launch.
+struct StepArgs {
+    int nx, ny, nz, pbx, pby, pbz;
+    int densratio, obstacles, write_u, zseg;
+    double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
+    double scale[NSCALE_H];
+    const void* min;
+    void* mout;
+    const void* uin;
+    void* uout;
+    const void* pin;
+    void* pout;
+    const int8_t* isf;
+    int* err;
+};
+
+using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
+
+// one table per storage type, defined in lbf_inst_<storage>.cu
+StepLauncher step_launcher_f32(int lat, int ho, int tc);
+StepLauncher step_launcher_f16(int lat, int ho, int tc);
+StepLauncher step_launcher_bf16(int lat, int ho, int tc);
+StepLauncher step_launcher_f64(int lat, int ho, int tc);
+
+// wetting tables (solid nodes whose ghost phi the reference updates)
+struct WetArgs {
+    int n;                    // entries
+    int nx, ny, nz, pbx, pby, pbz;
+    const long long* s_idx;   // solid node
+    const int* donor;         // 3 x n wrapped donor coordinates
+    const int* flag;          // WET_*
+    const double* wn;         // 3 x n unit wall normal
+    const int* shift;         // 3 x n link shift -c of the donor link
+    double cot_theta;
+    const void* pin;          // phi read (ghost before update, donor phi, donor stencil)
+    void* wout;               // new ghost values (n)
+    void* scatter_dst;        // phi buffer receiving scatter_src (or nullptr)
+    const void* scatter_src;  // ghost values of the previous step
+    int prime;                // integrator pre-loop call: aux = 0 and halos = 0
+};
+enum { WET_NORMAL = 0, WET_OUTSIDE = 1, WET_HIGHWRAP = 2 };
+
+cudaError_t launch_wetting(int storage, const WetArgs& a, cudaStream_t st);
+cudaError_t launch_wet_apply(int storage, int n, const long long* s_idx, const void* src, void* dst, cudaStream_t st);
+
+// host array <-> device field conversions
+cudaError_t launch_convert_in(int storage, bool is_phi, const void* src, int src_dtype, void* dst, long long n,
+                              double scale, cudaStream_t st);
+cudaError_t launch_convert_out(int storage, bool is_phi, const void* src, void* dst, int dst_dtype, long long n,
+                               double inv_scale, cudaStream_t st);
+
+// copy_print extraction
+struct PrintArgs {
+    long long N;
+    int mode;            // 0: P, 1: phi, 2: rho_phi
+    double rho_r, rho_b;
+    const void* P;       // moment field 0
+    const void* vel;     // 3 consecutive velocity fields
+    const void* phi;
+    double sP, su[3];    // inverse scales
+    float* rho;
+    float* vel_out;      // interleaved 3 x N
+    float* press;
+};
+cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
+
+// FP64 reductions over fluid nodes: out[5] = {sum phi, sum P, sum u, sum v, sum w}
+cudaError_t launch_reduce(int storage, long long N, const void* mom, const void* phi, const int8_t* isf,
+                          const double* inv_scale, double* d_out, cudaStream_t st);
+
+size_t storage_bytes(int storage);
+size_t phi_bytes(int storage);
+
+}  // namespace lbf

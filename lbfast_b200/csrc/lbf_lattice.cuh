@@ -1,0 +1,129 @@
+// lbf_lattice.cuh -- lattice constants and per-node arithmetic of the LBFAST
+// time step, written for the fused sm_100a kernel.
+//
+// Link order, weights and opposites follow the reference's tables
+// (vars_module.f90:319-338 for D3Q27, :666-684 for D3Q19), so that
+// populations, isfluid neighbour tests and bounce-back pairings line up with
+// the reference's.
+//
+// The post-collision population of the reference's fused kernel
+// (lb_cuda_fused_module.f90:637-713) is a Hermite expansion:
+//     f*_l = sum_r Minv_mrt(r,l) m*_r,   Minv_mrt(r,l) = w_l H_r(c_l) / <H_r,H_r>
+// with coefficients
+//     m*_0  = P
+//     m*_a  = u_a + F_a/2
+//     m*_ab = u_a u_b + (1-omega) Pn_ab + (u_a F_b + u_b F_a)/2
+//     m*_r  = eq_r(u) + (1-omega) neq_r(u,Pn)          r >= 10 (HIGHORDER)
+// where eq_r / neq_r are the monomials and recursive-regularisation terms the
+// reference writes out for rows 10..26 (lb_cuda_fused_module.f90:667-703).
+// On D3Q27 the expansion factorises over the three axes (D3Q27 = D1Q3^3),
+// so populations come from 27 coefficients by three passes of a 3-point
+// transform instead of a 27x27 product; D3Q19 uses the direct per-link form.
+#pragma once
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+namespace lbf {
+
+// D3Q27 link table (D3Q19 = first 19 entries)
+__host__ __device__ constexpr int EX(int l) {
+    constexpr int t[27] = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1,-1, 1, 1,-1};
+    return t[l];
+}
+__host__ __device__ constexpr int EY(int l) {
+    constexpr int t[27] = {0, 0, 0, 1,-1, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1,-1, 1,-1, 1};
+    return t[l];
+}
+__host__ __device__ constexpr int EZ(int l) {
+    constexpr int t[27] = {0, 0, 0, 0, 0, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1, 1,-1, 1,-1, 1,-1,-1, 1};
+    return t[l];
+}
+__host__ __device__ constexpr int OPP(int l) {
+    constexpr int t[27] = {0, 2, 1, 4, 3, 6, 5, 8, 7,10, 9,12,11,14,13,16,15,18,17,20,19,22,21,24,23,26,25};
+    return t[l];
+}
+// weight of link l; D3Q27: 8/27, 2/27, 1/54, 1/216; D3Q19: 1/3, 1/18, 1/36
+template <int LAT> __host__ __device__ constexpr double WL(int l) {
+    return LAT == 27 ? ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 8.0 / 27.0 :
+                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 2.0 / 27.0 :
+                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 2 ? 1.0 / 54.0 : 1.0 / 216.0)
+                     : ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 1.0 / 3.0 :
+                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+// link index of velocity (cx,cy,cz) in the D3Q27 ordering
+__host__ __device__ constexpr int LINK(int cx, int cy, int cz) {
+    int r = -1;
+    for (int l = 0; l < 27; ++l)
+        if (EX(l) == cx && EY(l) == cy && EZ(l) == cz) r = l;
+    return r;
+}
+
+template <typename R> __device__ __forceinline__ R fmaf_t(R a, R b, R c) { return fma(a, b, c); }
+
+// ---------------------------------------------------------------------------
+// storage codecs: fields live in HBM as S; arithmetic is in R.  Scaled 16-bit
+// storage keeps value*scale (scale per field, chosen on the host).
+// ---------------------------------------------------------------------------
+template <typename S> struct Codec;
+template <> struct Codec<float> {
+    static constexpr bool scaled = false;
+    template <typename R> __device__ static R ld(const float* p, long long i, R) { return (R)__ldg(p + i); }
+    template <typename R> __device__ static void st(float* p, long long i, R v, R) { p[i] = (float)v; }
+};
+template <> struct Codec<double> {
+    static constexpr bool scaled = false;
+    template <typename R> __device__ static R ld(const double* p, long long i, R) { return (R)__ldg(p + i); }
+    template <typename R> __device__ static void st(double* p, long long i, R v, R) { p[i] = (double)v; }
+};
+template <> struct Codec<__half> {
+    static constexpr bool scaled = true;
+    template <typename R> __device__ static R ld(const __half* p, long long i, R inv) {
+        return (R)__half2float(__ldg(p + i)) * inv;
+    }
+    template <typename R> __device__ static void st(__half* p, long long i, R v, R sc) {
+        p[i] = __float2half_rn((float)(v * sc));
+    }
+};
+template <> struct Codec<__nv_bfloat16> {
+    static constexpr bool scaled = true;
+    template <typename R> __device__ static R ld(const __nv_bfloat16* p, long long i, R inv) {
+        return (R)__bfloat162float(__ldg(p + i)) * inv;
+    }
+    template <typename R> __device__ static void st(__nv_bfloat16* p, long long i, R v, R sc) {
+        p[i] = __float2bfloat16_rn((float)(v * sc));
+    }
+};
+
+// phi keeps 32-bit storage when the moments are stored in 16 bits: it lives in
+// [0,1] and a 16-bit mantissa cannot resolve its interface profile.
+template <typename S> struct PhiStore { using type = S; };
+template <> struct PhiStore<__half> { using type = float; };
+template <> struct PhiStore<__nv_bfloat16> { using type = float; };
+
+// field slots of the per-field scale table
+enum : int { F_P = 0, F_U = 1, F_PXX = 4, F_UOLD = 10, F_PHI = 13, NSCALE = 14 };
+
+// ---------------------------------------------------------------------------
+// kernel parameters (by value)
+// ---------------------------------------------------------------------------
+template <typename S, typename R> struct StepParams {
+    int nx, ny, nz;
+    int pbx, pby, pbz;
+    long long plane;  // nx*ny
+    long long N;      // nx*ny*nz
+    int densratio, obstacles, write_u;
+    int zseg;         // planes per z segment
+    R omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
+    R scale[NSCALE], inv_scale[NSCALE];
+    const S* min;     // 10 x N moments, input
+    S* mout;          // 10 x N moments, output
+    const S* uin;     // 3 x N velocity of the previous step (DENSRATIO)
+    S* uout;          // 3 x N velocity after the force half-step
+    const typename PhiStore<S>::type* pin;  // N phase field, input
+    typename PhiStore<S>::type* pout;       // N phase field, output (fluid nodes)
+    const int8_t* isf;  // N isfluid (obstacles), else nullptr
+    int* err;         // device error word
+};
+
+}  // namespace lbf

@@ -1,0 +1,266 @@
+// lbf_misc.cu -- the small kernels around the fused step: wetting ghost phi,
+// field conversions at the host boundary, copy_print extraction and FP64
+// reductions.
+#include "lbf_internal.h"
+#include "lbf_stream.cuh"
+
+namespace lbf {
+
+size_t storage_bytes(int storage) {
+    switch (storage) {
+        case 0: return 4;
+        case 1: return 2;
+        case 2: return 2;
+        case 3: return 8;
+    }
+    return 0;
+}
+size_t phi_bytes(int storage) { return storage == 3 ? 8 : 4; }
+
+template <typename S> struct Arith { using R = float; };
+template <> struct Arith<double> { using R = double; };
+
+template <typename Fn> static cudaError_t by_storage(int storage, Fn&& fn) {
+    switch (storage) {
+        case 0: return fn(float{});
+        case 1: return fn(__half{});
+        case 2: return fn(__nv_bfloat16{});
+        case 3: return fn(double{});
+    }
+    return cudaErrorInvalidValue;
+}
+
+static inline int blocks_for(long long n, int bs) {
+    long long b = (n + bs - 1) / bs;
+    if (b > 148LL * 64) b = 148LL * 64;  // grid-stride beyond this
+    return (int)(b < 1 ? 1 : b);
+}
+
+// ---------------------------------------------------------------------------
+// Wetting ghost phi at solid nodes: PHI_int_boundary_kernel,
+// lb_cuda_boundary_module.f90:218-459.  The wall normal and the donor depend
+// only on isfluid and are precomputed on the host; here the donor's gradient
+// (compute_norm_interface at the donor, lb_cuda_auxfields_module.f90:72-112)
+// and the extrapolation (:404-454) are evaluated.  The result goes to `wout`
+// and is written into phi only after every reader of the pre-wetting phi has
+// run (see lbf_step).
+// ---------------------------------------------------------------------------
+template <typename SP, typename R>
+__global__ void wetting_kernel(const WetArgs a) {
+    using CP = Codec<SP>;
+    const SP* pin = static_cast<const SP*>(a.pin);
+    SP* wout = static_cast<SP*>(a.wout);
+    const long long plane = (long long)a.nx * a.ny;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        if (a.scatter_dst) {
+            static_cast<SP*>(a.scatter_dst)[a.s_idx[i]] = static_cast<const SP*>(a.scatter_src)[i];
+        }
+        const R old = CP::ld(pin, a.s_idx[i], R(1));
+        const int flag = a.flag[i];
+        R ghost;
+        if (flag == WET_OUTSIDE || (a.prime && flag == WET_HIGHWRAP)) {
+            // donor on a never-written halo layer: phi = 0 and aux = 0 there
+            ghost = R(0);
+        } else {
+            const int dx = a.donor[3 * i], dy = a.donor[3 * i + 1], dz = a.donor[3 * i + 2];
+            const R phid = CP::ld(pin, (long long)dz * plane + (long long)dy * a.nx + dx, R(1));
+            R gx = 0, gy = 0, gz = 0;
+            if (!a.prime) {
+                auto A = [&](int ox, int oy, int oz) -> R {
+                    bool ok = true;
+                    int x = wrap_coord(dx + ox, a.nx, a.pbx, ok);
+                    int y = wrap_coord(dy + oy, a.ny, a.pby, ok);
+                    int z = wrap_coord(dz + oz, a.nz, a.pbz, ok);
+                    return ok ? CP::ld(pin, (long long)z * plane + (long long)y * a.nx + x, R(1)) : R(0);
+                };
+                R g0, g1, g2;
+                iso_grad<R>(A, g0, g1, g2);
+                R mg = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+                R den = mg + R(1.0e-9);
+                gx = (g0 / den) * mg;
+                gy = (g1 / den) * mg;
+                gz = (g2 / den) * mg;
+            }
+            const R wx = (R)a.wn[3 * i], wy = (R)a.wn[3 * i + 1], wz = (R)a.wn[3 * i + 2];
+            const R gdw = gx * wx + gy * wy + gz * wz;
+            const R tx = gx - gdw * wx, ty = gy - gdw * wy, tz = gz - gdw * wz;
+            const R tmag = sqrt(tx * tx + ty * ty + tz * tz);
+            const R dn = -tmag * (R)a.cot_theta;
+            const R bx = tx + dn * wx, by = ty + dn * wy, bz = tz + dn * wz;
+            const R sx = (R)a.shift[3 * i], sy = (R)a.shift[3 * i + 1], sz = (R)a.shift[3 * i + 2];
+            ghost = phid + (bx * sx + by * sy + bz * sz) * (R(4) * old * (R(1) - old));
+        }
+        ghost = max(R(0), min(R(1), ghost));
+        CP::st(wout, i, ghost, R(1));
+    }
+}
+
+cudaError_t launch_wetting(int storage, const WetArgs& a, cudaStream_t st) {
+    if (a.n <= 0) return cudaSuccess;
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        using SP = typename PhiStore<S>::type;
+        using R = typename Arith<S>::R;
+        wetting_kernel<SP, R><<<blocks_for(a.n, 256), 256, 0, st>>>(a);
+        return cudaGetLastError();
+    });
+}
+
+template <typename SP>
+__global__ void wet_apply_kernel(int n, const long long* s_idx, const SP* src, SP* dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[s_idx[i]] = src[i];
+}
+
+cudaError_t launch_wet_apply(int storage, int n, const long long* s_idx, const void* src, void* dst, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        using SP = typename PhiStore<S>::type;
+        wet_apply_kernel<SP><<<blocks_for(n, 256), 256, 0, st>>>(n, s_idx, static_cast<const SP*>(src),
+                                                                   static_cast<SP*>(dst));
+        return cudaGetLastError();
+    });
+}
+
+// ---------------------------------------------------------------------------
+// conversions between host arrays (float/double) and stored fields
+// ---------------------------------------------------------------------------
+template <typename T, typename S, typename R>
+__global__ void convert_in_kernel(const T* src, S* dst, long long n, R scale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        Codec<S>::st(dst, i, (R)src[i], scale);
+}
+template <typename S, typename T, typename R>
+__global__ void convert_out_kernel(const S* src, T* dst, long long n, R inv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (T)Codec<S>::ld(src, i, inv);
+}
+
+cudaError_t launch_convert_in(int storage, bool is_phi, const void* src, int src_dtype, void* dst, long long n,
+                              double scale, cudaStream_t st) {
+    return by_storage(storage, [&](auto tag) {
+        using S0 = decltype(tag);
+        using R = typename Arith<S0>::R;
+        auto go = [&](auto stag) {
+            using S = decltype(stag);
+            if (src_dtype == 1)
+                convert_in_kernel<double, S, R><<<blocks_for(n, 256), 256, 0, st>>>(static_cast<const double*>(src),
+                                                                                    static_cast<S*>(dst), n, (R)scale);
+            else
+                convert_in_kernel<float, S, R><<<blocks_for(n, 256), 256, 0, st>>>(static_cast<const float*>(src),
+                                                                                   static_cast<S*>(dst), n, (R)scale);
+            return cudaGetLastError();
+        };
+        if (is_phi) return go(typename PhiStore<S0>::type{});
+        return go(S0{});
+    });
+}
+
+cudaError_t launch_convert_out(int storage, bool is_phi, const void* src, void* dst, int dst_dtype, long long n,
+                               double inv_scale, cudaStream_t st) {
+    return by_storage(storage, [&](auto tag) {
+        using S0 = decltype(tag);
+        using R = typename Arith<S0>::R;
+        auto go = [&](auto stag) {
+            using S = decltype(stag);
+            if (dst_dtype == 1)
+                convert_out_kernel<S, double, R><<<blocks_for(n, 256), 256, 0, st>>>(
+                    static_cast<const S*>(src), static_cast<double*>(dst), n, (R)inv_scale);
+            else
+                convert_out_kernel<S, float, R><<<blocks_for(n, 256), 256, 0, st>>>(
+                    static_cast<const S*>(src), static_cast<float*>(dst), n, (R)inv_scale);
+            return cudaGetLastError();
+        };
+        if (is_phi) return go(typename PhiStore<S0>::type{});
+        return go(S0{});
+    });
+}
+
+// ---------------------------------------------------------------------------
+// copy_print (print_module.f90:638-776)
+// ---------------------------------------------------------------------------
+template <typename S, typename R>
+__global__ void print_kernel(const PrintArgs a) {
+    using SP = typename PhiStore<S>::type;
+    const S* P = static_cast<const S*>(a.P);
+    const S* V = static_cast<const S*>(a.vel);
+    const SP* ph = static_cast<const SP*>(a.phi);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
+        R press = Codec<S>::ld(P, i, (R)a.sP);
+        if (a.rho) {
+            R r;
+            if (a.mode == 0) r = press;
+            else {
+                R f = Codec<SP>::ld(ph, i, R(1));
+                r = a.mode == 1 ? f : (R)a.rho_r * f + (R(1) - f) * (R)a.rho_b;
+            }
+            a.rho[i] = (float)r;
+        }
+        if (a.press) a.press[i] = (float)press;
+        if (a.vel_out) {
+            a.vel_out[3 * i + 0] = (float)Codec<S>::ld(V, i, (R)a.su[0]);
+            a.vel_out[3 * i + 1] = (float)Codec<S>::ld(V, a.N + i, (R)a.su[1]);
+            a.vel_out[3 * i + 2] = (float)Codec<S>::ld(V, 2 * a.N + i, (R)a.su[2]);
+        }
+    }
+}
+
+cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st) {
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        using R = typename Arith<S>::R;
+        print_kernel<S, R><<<blocks_for(a.N, 256), 256, 0, st>>>(a);
+        return cudaGetLastError();
+    });
+}
+
+// ---------------------------------------------------------------------------
+// FP64 sums over fluid nodes (phi_sum_count_kernel, lb_cuda_boundary_module.f90:461-515,
+// with a block-level tree instead of one atomic per node)
+// ---------------------------------------------------------------------------
+template <typename S>
+__global__ void reduce_kernel(long long N, const S* mom, const typename PhiStore<S>::type* phi, const int8_t* isf,
+                              double s0, double s1, double s2, double s3, double* out) {
+    using SP = typename PhiStore<S>::type;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        if (isf) {
+            int f = isf[i];
+            if (f != 1 && f != -1) continue;
+        }
+        if (phi) acc[0] += (double)Codec<SP>::ld(phi, i, 1.0);
+        acc[1] += (double)Codec<S>::ld(mom, i, s0);
+        acc[2] += (double)Codec<S>::ld(mom, N + i, s1);
+        acc[3] += (double)Codec<S>::ld(mom, 2 * N + i, s2);
+        acc[4] += (double)Codec<S>::ld(mom, 3 * N + i, s3);
+    }
+    __shared__ double red[5][256];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+#pragma unroll
+            for (int k = 0; k < 5; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) atomicAdd(out + k, red[k][0]);
+}
+
+cudaError_t launch_reduce(int storage, long long N, const void* mom, const void* phi, const int8_t* isf,
+                          const double* inv_scale, double* d_out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 5 * sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        using SP = typename PhiStore<S>::type;
+        reduce_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(N, static_cast<const S*>(mom),
+                                                              static_cast<const SP*>(phi), isf, inv_scale[0],
+                                                              inv_scale[1], inv_scale[2], inv_scale[3], d_out);
+        return cudaGetLastError();
+    });
+}
+
+}  // namespace lbf

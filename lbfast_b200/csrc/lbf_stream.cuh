@@ -1,0 +1,116 @@
+// lbf_stream.cuh -- the fused LBFAST time step for sm_100a.
+//
+// One launch performs what the reference does in five kernels plus four
+// halo copies per half-step (integrator_module.f90:270-544):
+//   compute_norm_interface (lb_cuda_auxfields_module.f90:19-139)
+//   compute_div_theta_n    (lb_cuda_auxfields_module.f90:1085-1164)
+//   moments_LB             (lb_cuda_moments_module.f90:19-341)
+//   fused_LB collide+stream(lb_cuda_fused_module.f90:426-750)
+//   update_phifields       (lb_cuda_update_phi_module.f90:19-104)
+//   LB_int_boundary        (lb_cuda_boundary_module.f90:19-216)
+//   exchange_*_intpbc      (mpi_module.f90:2203-3286) -> periodic index wrap
+//
+// Work decomposition.  A CTA owns a TX x TY column of the box and sweeps a
+// segment of z planes.  For collision plane q it keeps in shared memory
+//   phi   planes q-1..q+3 on the tile + 3-node ring   (5-slot ring)
+//   theta = phi(1-phi) n and g~ = n|grad phi| for planes q-1..q+1 on the
+//           tile + 2-node ring                          (3-slot ring)
+//   post-collision populations of plane q on the tile + 1-node ring.
+// Each output node then pulls f*_l(x - c_l) from shared memory: the nine
+// (cx,cy) populations of each cz slice of plane q go to output plane q+cz,
+// accumulated in registers; plane q-1 is complete after plane q and is
+// written out.  Halo nodes are recomputed instead of exchanged, so one step
+// reads the moments, the previous velocity and phi once and writes them once
+// (plus halo rereads that hit L2).
+//
+// Non-periodic directions: nodes outside the box carry isfluid = 1 and zero
+// fields, as the reference's never-written halo layers do.
+#pragma once
+#include "lbf_lattice.cuh"
+
+namespace lbf {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int R1X = TX + 2, R1Y = TY + 2, R1N = R1X * R1Y;  // collision region
+constexpr int R2X = TX + 4, R2Y = TY + 4, R2N = R2X * R2Y;  // theta region
+constexpr int R3X = TX + 6, R3Y = TY + 6, R3N = R3X * R3Y;  // phi region
+constexpr int NRING1 = R1N - NT;                              // 84 ring nodes of R1
+constexpr int PHI_SLOTS = 5, TH_SLOTS = 3, TH_COMP = 6;
+
+template <int LAT, bool TC, typename R> constexpr size_t stream_smem_bytes() {
+    return sizeof(R) * (size_t(LAT) * R1N + (TC ? size_t(PHI_SLOTS) * R3N + size_t(TH_SLOTS) * TH_COMP * R2N : 0));
+}
+
+__device__ __forceinline__ int wrap_coord(int g, int n, int periodic, bool& ok) {
+    if (g < 0) {
+        if (periodic) { g = g % n; if (g < 0) g += n; } else ok = false;
+    } else if (g >= n) {
+        if (periodic) g = g % n; else ok = false;
+    }
+    return g;
+}
+
+// D3Q27 isotropic gradient of the reference (lb_cuda_auxfields_module.f90:72-100),
+// always with D3Q27 weights.  a(i,j,k) reads phi at offset (i,j,k).
+template <typename R, typename A> __device__ __forceinline__ void iso_grad(const A& a, R& gx, R& gy, R& gz) {
+    const R p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
+    gx = R(3) * (p1 * (a(1, 0, 0) - a(-1, 0, 0)) +
+                 p2 * ((a(1, 1, 0) - a(-1, -1, 0)) + (a(1, -1, 0) - a(-1, 1, 0)) +
+                       (a(1, 0, 1) - a(-1, 0, -1)) + (a(1, 0, -1) - a(-1, 0, 1))) +
+                 p3 * ((a(1, 1, 1) - a(-1, -1, -1)) + (a(1, -1, -1) - a(-1, 1, 1)) +
+                       (a(1, -1, 1) - a(-1, 1, -1)) + (a(1, 1, -1) - a(-1, -1, 1))));
+    gy = R(3) * (p1 * (a(0, 1, 0) - a(0, -1, 0)) +
+                 p2 * ((a(1, 1, 0) - a(-1, -1, 0)) + (a(-1, 1, 0) - a(1, -1, 0)) +
+                       (a(0, 1, 1) - a(0, -1, -1)) + (a(0, 1, -1) - a(0, -1, 1))) +
+                 p3 * ((a(1, 1, 1) - a(-1, -1, -1)) + (a(-1, 1, -1) - a(1, -1, 1)) +
+                       (a(1, 1, -1) - a(-1, -1, 1)) + (a(-1, 1, 1) - a(1, -1, -1))));
+    gz = R(3) * (p1 * (a(0, 0, 1) - a(0, 0, -1)) +
+                 p2 * ((a(1, 0, 1) - a(-1, 0, -1)) + (a(-1, 0, 1) - a(1, 0, -1)) +
+                       (a(0, 1, 1) - a(0, -1, -1)) + (a(0, -1, 1) - a(0, 1, -1))) +
+                 p3 * ((a(1, 1, 1) - a(-1, -1, -1)) + (a(-1, -1, 1) - a(1, 1, -1)) +
+                       (a(1, -1, 1) - a(-1, 1, -1)) + (a(-1, 1, 1) - a(1, -1, -1))));
+}
+
+// isotropic Laplacian (lb_cuda_auxfields_module.f90:121-135)
+template <typename R, typename A> __device__ __forceinline__ R iso_lap(const A& a) {
+    const R p0 = R(8.0 / 27.0), p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
+    return R(6) * (a(0, 0, 0) * (p0 - R(1)) +
+                   (p1 * (a(1, 0, 0) + a(-1, 0, 0) + a(0, 1, 0) + a(0, -1, 0) + a(0, 0, 1) + a(0, 0, -1)) +
+                    p2 * ((a(1, 1, 0) + a(-1, -1, 0)) + (a(1, -1, 0) + a(-1, 1, 0)) + (a(1, 0, 1) + a(-1, 0, -1)) +
+                          (a(1, 0, -1) + a(-1, 0, 1)) + (a(0, 1, 1) + a(0, -1, -1)) + (a(0, 1, -1) + a(0, -1, 1))) +
+                    p3 * ((a(1, 1, 1) + a(-1, -1, -1)) + (a(1, -1, -1) + a(-1, 1, 1)) + (a(1, -1, 1) + a(-1, 1, -1)) +
+                          (a(1, 1, -1) + a(-1, -1, 1)))));
+}
+
+// divergence of theta (lb_cuda_auxfields_module.f90:1136-1157)
+template <typename R, typename AX, typename AY, typename AZ>
+__device__ __forceinline__ R iso_div(const AX& X, const AY& Y, const AZ& Z) {
+    const R p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
+    R dx = p1 * (X(1, 0, 0) - X(-1, 0, 0)) +
+           p2 * ((X(1, 1, 0) - X(-1, -1, 0)) + (X(1, -1, 0) - X(-1, 1, 0)) + (X(1, 0, 1) - X(-1, 0, -1)) +
+                 (X(1, 0, -1) - X(-1, 0, 1))) +
+           p3 * ((X(1, 1, 1) - X(-1, -1, -1)) + (X(1, -1, -1) - X(-1, 1, 1)) + (X(1, -1, 1) - X(-1, 1, -1)) +
+                 (X(1, 1, -1) - X(-1, -1, 1)));
+    R dy = p1 * (Y(0, 1, 0) - Y(0, -1, 0)) +
+           p2 * ((Y(1, 1, 0) - Y(-1, -1, 0)) + (Y(-1, 1, 0) - Y(1, -1, 0)) + (Y(0, 1, 1) - Y(0, -1, -1)) +
+                 (Y(0, 1, -1) - Y(0, -1, 1))) +
+           p3 * ((Y(1, 1, 1) - Y(-1, -1, -1)) + (Y(-1, 1, -1) - Y(1, -1, 1)) + (Y(1, 1, -1) - Y(-1, -1, 1)) +
+                 (Y(-1, 1, 1) - Y(1, -1, -1)));
+    R dz = p1 * (Z(0, 0, 1) - Z(0, 0, -1)) +
+           p2 * ((Z(1, 0, 1) - Z(-1, 0, -1)) + (Z(-1, 0, 1) - Z(1, 0, -1)) + (Z(0, 1, 1) - Z(0, -1, -1)) +
+                 (Z(0, -1, 1) - Z(0, 1, -1))) +
+           p3 * ((Z(1, 1, 1) - Z(-1, -1, -1)) + (Z(-1, -1, 1) - Z(1, 1, -1)) + (Z(1, -1, 1) - Z(-1, 1, -1)) +
+                 (Z(-1, 1, 1) - Z(1, -1, -1)));
+    return (dx + dy + dz) * R(3);
+}
+
+// 1-D D1Q3 inverse transform: Hermite coefficients (m0, m1, m2) -> values at c = -1, 0, +1
+template <typename R> __device__ __forceinline__ void d1q3_inv(R m0, R m1, R m2, R& vm, R& v0, R& vp) {
+    R s = fmaf_t(m0, R(1.0 / 6.0), R(0.5) * m2);
+    R d = R(0.5) * m1;
+    vm = s - d;
+    vp = s + d;
+    v0 = fmaf_t(m0, R(2.0 / 3.0), -m2);
+}
+
+}  // namespace lbf
