@@ -1,0 +1,316 @@
+"""Benchmark of the LBFAST time step on B200.
+
+Workload (the reference's Laplace check, the configuration its headline
+metric is quoted on that fits one GPU): two-component DENSRATIO D3Q27
+HIGHORDER, 256^3 periodic, FP32, a centred droplet R=40 with the
+fcut_tanh profile of width 3, density ratio 100 (rho_r = 1, rho_b = 0.01),
+sigma = 0.03, nu1 = nu2 = 0.1, tau_diff = 0.1, fluids at rest.  Synthetic
+input generated in-process (no dataset exists for this path).
+
+One "step" is one LB time step of the whole box.  The timed region covers
+exactly --steps steps between barriers and device synchronisations, timed with
+CUDA events on the launching stream (max over ranks).  The state (1.9 GB)
+exceeds the 126 MB L2, so no flush is needed between steps.
+
+Arms:
+  default          this library, device-resident state ("value"), plus an
+                   end-to-end run through the C ABI from pinned host buffers
+                   ("e2e": initial state uploaded, steps, copy_print read back)
+  --impl reference the reference's algorithm on the host cores: the C
+                   restatement in oracle/ (the reference itself is CUDA
+                   Fortran/OpenACC and cannot be built here), FP32, all host
+                   threads, on a bounded number of steps of the same box.
+
+Multi-GPU (torchrun): every rank advances its own replica of the box (the
+single-GPU path has no exchange step); "value" sums the ranks' lattice
+updates over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS (D3Q27 high-order two-component lattice updates per second)"
+UNIT = "MLUPS"
+LBOX = 256
+B_LUP = {"f32": 112, "f16": 60, "bf16": 60, "f64": 224}  # algorithmic bytes per lattice update
+
+
+def workload(storage: str = "f32", L: int = LBOX):
+    import lbfast_b200 as lbf
+    p = lbf.Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1,
+                   visc1=0.1, visc2=0.1, rho_r=1.0, rho_b=0.01, sigma=0.03, width=3.0, tau_diff=0.1,
+                   printphi=1, storage=storage)
+    R = 40.0 * L / 256
+    m, phi = lbf.ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, 1.0, 0.01, True)
+    return p, m, phi
+
+
+def config_dict(storage, L=LBOX):
+    return {"workload": f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO (100:1), "
+                        f"R={int(40 * L / 256)}, width 3, sigma 0.03",
+            "box": [L, L, L], "lattice": "D3Q27", "highorder": True, "twocomponent": True, "densratio": True,
+            "storage": storage, "bytes_per_lup": B_LUP[storage],
+            "l2_policy": "state (%.2f GB) larger than the 126 MB L2; no flush" % (L ** 3 * B_LUP[storage] / 1e9)}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="lbf_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[2:]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, local, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args, rank, local, world):
+    import numpy as np
+    import torch
+
+    import lbfast_b200 as lbf
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    p, m, phi = workload(args.storage, args.box)
+    N = p.lx * p.ly * p.lz
+    s = lbf.Solver(p)
+    s.set_stream(stream.cuda_stream)
+    s.set_fields(m, phi)
+    s.step(args.warmup)
+    s.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = allmax(e0.elapsed_time(e1), world)
+    clocks = clk.summary()
+    ms_step = ms / args.steps
+    value = world * N * args.steps / (ms * 1e-3) / 1e6
+    # the step kernel is the only launch per step: its average duration is the step time
+    bytes_launch = B_LUP[args.storage] * N
+    achieved = bytes_launch / (ms_step * 1e-3) / 1e9
+    red = s.reduce()
+    ok = bool(np.all(np.isfinite(red)))
+    s.close()
+
+    # end to end through the C ABI with pinned host buffers
+    pin_m = torch.empty((10, p.lz, p.ly, p.lx), dtype=torch.float32, pin_memory=True)
+    pin_phi = torch.empty((p.lz, p.ly, p.lx), dtype=torch.float32, pin_memory=True)
+    pin_m.numpy()[...] = m
+    pin_phi.numpy()[...] = phi
+    rho = torch.empty((p.lz, p.ly, p.lx), dtype=torch.float32, pin_memory=True).numpy()
+    vel = torch.empty((p.lz, p.ly, p.lx, 3), dtype=torch.float32, pin_memory=True).numpy()
+    press = torch.empty((p.lz, p.ly, p.lx), dtype=torch.float32, pin_memory=True).numpy()
+    s = lbf.Solver(p)
+    s.set_stream(stream.cuda_stream)
+    import ctypes as C
+    lib = lbf.load()
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    # warm the path once (allocations of the staging buffer)
+    lbf.capi.check(lib.lbf_set_fields(s.h, C.c_void_p(pin_m.data_ptr()), C.c_void_p(pin_phi.data_ptr()), 0))
+    s.step(1)
+    lbf.capi.check(lib.lbf_get_print_fields(s.h, fp(rho), fp(vel), fp(press)))
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    lbf.capi.check(lib.lbf_set_fields(s.h, C.c_void_p(pin_m.data_ptr()), C.c_void_p(pin_phi.data_ptr()), 0))
+    s.step(args.steps)
+    lbf.capi.check(lib.lbf_get_print_fields(s.h, fp(rho), fp(vel), fp(press)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(world)
+    ms_e2e = allmax(max(e0.elapsed_time(e1), wall * 1e3), world)
+    s.close()
+    h2d = (10 + 1) * N * 4
+    d2h = 5 * N * 4
+    e2e = {"value": world * N * args.steps / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "path": "lbf_set_fields (pinned host, f32) + lbf_step + lbf_get_print_fields; the initial state is "
+                   "uploaded once and copy_print read back once per run, the reference's stamp = nsteps cadence"}
+    return {"value": value, "ms": ms, "ms_step": ms_step, "achieved": achieved, "clocks": clocks, "e2e": e2e,
+            "finite": ok}
+
+
+def cpu_baseline(storage: str, L: int, nsteps: int, threads: int):
+    """The oracle (C restatement of the reference, FP32 build stand-in) on the
+    host cores: `nsteps` steps of the same box."""
+    import numpy as np
+    from oracle import oracle as O
+    p, m, phi = workload(storage, L)
+    O.set_threads(threads)
+    o = O.Oracle(p.oracle_dict(), "f32")
+    o.set_isfluid(np.ones(p.shape, np.int8))
+    o.set_fields(m, phi)
+    o.step(0)
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    dt = time.perf_counter() - t0
+    return p.lx * p.ly * p.lz * nsteps / dt / 1e6, dt
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--box", type=int, default=LBOX)
+    ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, local, world = dist_init()
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # each timed step of the reference arm is one full oracle step of the box
+        for _ in range(min(args.warmup, 1)):
+            cpu_baseline(args.storage, args.box, 1, threads)
+        k = max(1, min(args.steps, 20))
+        mlups, dt = cpu_baseline(args.storage, args.box, k, threads)
+        line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": k, "warmup": min(args.warmup, 1), "ms_per_step": dt / k * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict(args.storage, args.box),
+                "cpu_baseline": {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{k} steps of the {args.box}^3 box, FP32 C restatement of the "
+                                           f"reference kernels (oracle/lbf_oracle.c), OpenMP over z"},
+                "e2e": {"value": mlups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    r = run_ours(args, rank, local, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mlups, dt = cpu_baseline(args.storage, args.box, args.cpu_steps, threads)
+        cpu = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_steps} steps of the same {args.box}^3 box ({dt:.1f} s), FP32 C restatement of "
+                         f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
+    if rank != 0:
+        return
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = _json.load(open(tpath)).get(f"{args.storage}_{args.box}")
+        except (OSError, ValueError):
+            traffic = None
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64", "data": "synthetic",
+        "config": dict(config_dict(args.storage, args.box), parallelism=f"replicas x{world}"),
+        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": peak, "unit": "GB/s",
+                     "frac": r["achieved"] / peak, "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "lbf::stream_kernel<27,HO,TC>", "bytes_per_launch": B_LUP[args.storage] * args.box ** 3},
+        "e2e": r["e2e"], "gpu_launches": args.steps, "clocks": r["clocks"], "cpu_baseline": cpu,
+        "finite": r["finite"],
+    }
+    print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

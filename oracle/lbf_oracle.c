@@ -53,6 +53,16 @@ typedef REAL real;
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#if defined(__x86_64__) || defined(__i386__)
+#include <xmmintrin.h>
+/* Flush-to-zero / denormals-are-zero during a step, as an x86 host build with
+ * nvfortran's default -Mflushz runs: at rest the high-order terms multiply up
+ * to six tiny velocities, and subnormal arithmetic on x86 is two orders of
+ * magnitude slower.  Set in every OpenMP thread (MXCSR is per thread). */
+#define FTZ_ON() _mm_setcsr(_mm_getcsr() | 0x8040)
+#else
+#define FTZ_ON() ((void)0)
+#endif
 
 typedef struct orc_params {
     int lx, ly, lz;
@@ -843,8 +853,22 @@ static void one_step(orc_state *s)
 void orc_step(orc_state *s, int nsteps)
 {
     int n;
+    unsigned int saved = 0;
+#if defined(__x86_64__) || defined(__i386__)
+    saved = _mm_getcsr();
+#endif
+#pragma omp parallel
+    FTZ_ON();
+    FTZ_ON();
     if (!s->primed) prime(s);
     for (n = 0; n < nsteps; n++) one_step(s);
+#if defined(__x86_64__) || defined(__i386__)
+    _mm_setcsr(saved);
+#pragma omp parallel
+    _mm_setcsr(saved);
+#else
+    (void)saved;
+#endif
 }
 
 void orc_set_threads(int n)

@@ -97,6 +97,7 @@ def test_split_calls_equal_one_call():
     b.step(12)
     ma, pa, ua = a.get_fields()
     mb, pb, ub = b.get_fields()
-    assert np.array_equal(ma, mb) and np.array_equal(pa, pb) and np.array_equal(ua, ub)
+    # interior solid nodes keep the reference's 0/0 seed (NaN); they are equal as NaN
+    assert np.array_equal(ma, mb) and np.array_equal(pa, pb, equal_nan=True) and np.array_equal(ua, ub)
     a.close()
     b.close()
