@@ -11,7 +11,7 @@ template <int LAT, bool HO, bool TC, typename S, typename R>
 cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     using SP = typename PhiStore<S>::type;
     static bool attr_set = false;
-    const size_t smem = stream_smem_bytes<LAT, TC, R>();
+    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

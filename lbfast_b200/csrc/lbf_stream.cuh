@@ -13,8 +13,9 @@
 // Work decomposition.  A CTA owns a TX x TY column of the box and sweeps a
 // segment of z planes.  For collision plane q it keeps in shared memory
 //   phi   planes q-1..q+3 on the tile + 3-node ring   (5-slot ring)
-//   theta = phi(1-phi) n and g~ = n|grad phi| for planes q-1..q+1 on the
-//           tile + 2-node ring                          (3-slot ring)
+//   theta = phi(1-phi) n on the tile + 2-node ring and g~ = n|grad phi| on
+//           the tile + 1-node ring, planes q-1..q+2   (4-slot ring)
+//   the moments (and u_old) of plane q staged by cp.async
 //   post-collision populations of plane q on the tile + 1-node ring.
 // Each output node then pulls f*_l(x - c_l) from shared memory: the nine
 // (cx,cy) populations of each cz slice of plane q go to output plane q+cz,
@@ -35,11 +36,7 @@ constexpr int R1X = TX + 2, R1Y = TY + 2, R1N = R1X * R1Y;  // collision region
 constexpr int R2X = TX + 4, R2Y = TY + 4, R2N = R2X * R2Y;  // theta region
 constexpr int R3X = TX + 6, R3Y = TY + 6, R3N = R3X * R3Y;  // phi region
 constexpr int NRING1 = R1N - NT;                              // 84 ring nodes of R1
-constexpr int PHI_SLOTS = 5, TH_SLOTS = 3, TH_COMP = 6;
-
-template <int LAT, bool TC, typename R> constexpr size_t stream_smem_bytes() {
-    return sizeof(R) * (size_t(LAT) * R1N + (TC ? size_t(PHI_SLOTS) * R3N + size_t(TH_SLOTS) * TH_COMP * R2N : 0));
-}
+constexpr int PHI_SLOTS = 5, TH_SLOTS4 = 4;
 
 __device__ __forceinline__ int wrap_coord(int g, int n, int periodic, bool& ok) {
     if (g < 0) {

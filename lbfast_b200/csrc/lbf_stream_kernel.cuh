@@ -1,15 +1,23 @@
 // lbf_stream_kernel.cuh -- body of the fused step kernel (see lbf_stream.cuh).
+//
+// Per z plane q a CTA runs two barrier phases:
+//   phase 1  theta(q+2) on the theta region, and the moments prologue +
+//            collision of plane q on the collision region (populations to
+//            shared memory).  The two sets of work are independent, so one
+//            barrier covers both, and the halo-ring collisions are placed on
+//            the warps with the least theta work.
+//   phase 2  asynchronous copies (cp.async) of the next plane's moments /
+//            u_old into a shared staging area and of phi(q+4) into its ring
+//            slot; then every output node pulls the populations of plane q
+//            and plane q-1 is written.  The copies complete behind this phase.
 #pragma once
 #include "lbf_stream.cuh"
 
 namespace lbf {
 
-// Per-node state after the moments prologue (lb_cuda_moments_module.f90:104-339).
-template <typename R> struct NodeState {
-    R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;  // post-prologue moments
-    R Fx, Fy, Fz;                                // force / rho_phi, as the collision reads it
-    R omega;
-};
+template <typename R> __device__ __forceinline__ R rcp(R x);
+template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ double rcp<double>(double x) { return 1.0 / x; }
 
 template <typename R>
 __device__ __forceinline__ void accum_slice(R (&acc)[10], R cz, R Y00, R Y01, R Y02, R Y10, R Y11, R Y20) {
@@ -25,15 +33,42 @@ __device__ __forceinline__ void accum_slice(R (&acc)[10], R cz, R Y00, R Y01, R 
     acc[9] += cz * Y01;
 }
 
+// asynchronous global -> shared copies of 4 or 8 bytes
+template <int BYTES> __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (BYTES == 4) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// fields staged per collision node: 10 moments (+3 u_old with a density ratio)
+constexpr int NSTAGE = 13;
+
+// 32/64-bit storage is prefetched with cp.async; 16-bit storage is read at the point of use
+template <typename S> constexpr bool staged() { return sizeof(S) >= 4; }
+
+template <int LAT, bool TC, typename S, typename R> constexpr size_t stream_smem_bytes_v2() {
+    size_t b = sizeof(R) * size_t(LAT) * R1N;
+    if (TC) b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(TH_SLOTS4) * (3 * R2N + 3 * R1N));
+    if (staged<S>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
+    return b;
+}
+
 template <int LAT, bool HO, bool TC, typename S, typename R>
-__global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p) {
+__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(const StepParams<S, R> p) {
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
     using CP = Codec<SP>;
+    constexpr bool STG = staged<S>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* pops = reinterpret_cast<R*>(smem_raw);  // [LAT][R1N]
-    R* phis = pops + LAT * R1N;                // [PHI_SLOTS][R3N]          (TC)
-    R* ths = phis + PHI_SLOTS * R3N;           // [TH_SLOTS][TH_COMP][R2N]  (TC)
+    R* pops = reinterpret_cast<R*>(smem_raw);          // [LAT][R1N]
+    R* phis = pops + LAT * R1N;                        // [PHI_SLOTS][R3N]     (TC)
+    R* ths = phis + (TC ? PHI_SLOTS * R3N : 0);        // [TH_SLOTS4][3][R2N]  (TC) theta
+    R* gts = ths + (TC ? TH_SLOTS4 * 3 * R2N : 0);     // [TH_SLOTS4][3][R1N]  (TC) g~
+    S* stg = reinterpret_cast<S*>(gts + (TC ? TH_SLOTS4 * 3 * R1N : 0));  // [NSTAGE][R1N] (STG)
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
@@ -47,14 +82,17 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
     const R cssq = R(1.0 / 3.0);
 
     // ---- static per-thread node tables (x/y wrap does not change along z) ----
-    // R1 node of pass 0 (tile interior) and pass 1 (ring of the collision region)
-    const int r1n0 = (ty + 1) * R1X + (tx + 1);
-    int r1n1 = -1;
-    if (t < NRING1) {
-        if (t < R1X) r1n1 = t;                                       // top row
-        else if (t < 2 * R1X) r1n1 = (R1Y - 1) * R1X + (t - R1X);    // bottom row
-        else if (t < 2 * R1X + TY) r1n1 = (t - 2 * R1X + 1) * R1X;   // left column
-        else r1n1 = (t - 2 * R1X - TY + 1) * R1X + (R1X - 1);        // right column
+    // collision nodes: A = tile interior node t; B = ring node for the last NRING1 threads
+    const int nodeA = (ty + 1) * R1X + (tx + 1);
+    int nodeB = -1;
+    {
+        const int r = t - (NT - NRING1);
+        if (r >= 0) {
+            if (r < R1X) nodeB = r;                                        // top row
+            else if (r < 2 * R1X) nodeB = (R1Y - 1) * R1X + (r - R1X);     // bottom row
+            else if (r < 2 * R1X + TY) nodeB = (r - 2 * R1X + 1) * R1X;    // left column
+            else nodeB = (r - 2 * R1X - TY + 1) * R1X + (R1X - 1);         // right column
+        }
     }
     auto r1_geom = [&](int node, int& off) -> bool {
         if (node < 0) { off = 0; return false; }
@@ -65,15 +103,14 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
         off = ok ? gy * nx + gx : 0;
         return ok;
     };
-    int r1off0, r1off1;
-    const bool r1ok0 = r1_geom(r1n0, r1off0);
-    const bool r1ok1 = r1_geom(r1n1, r1off1);
-    // output node of this thread
+    int offA, offB;
+    const bool okA = r1_geom(nodeA, offA);
+    const bool okB = r1_geom(nodeB, offB);
     const int ox = X0 + tx, oy = Y0 + ty;
     const bool out_ok = (ox < nx) && (oy < ny);
     const long long out_off = (long long)oy * nx + ox;
 
-    // neighbour x / y offsets of the output node, for the bounce-back isfluid tests
+    // neighbour x / y coordinates of the output node (bounce-back isfluid tests)
     int nbx[3], nby[3];
     bool nbx_ok[3], nby_ok[3];
 #pragma unroll
@@ -85,6 +122,7 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
         nby_ok[d] = oky;
     }
 
+    // theta nodes (R2): t and t + NT; phi nodes (R3): t, t + NT, t + 2 NT
     int r2_off[2] = {0, 0};
     bool r2_ok[2] = {false, false};
     int r3_off[3] = {0, 0, 0};
@@ -117,41 +155,69 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
     }
 
     auto zwrap = [&](int q, bool& ok) { return wrap_coord(q, nz, p.pbz, ok); };
-    auto phi_slot = [&](int q) { return (q - z0 + 3 + 5 * PHI_SLOTS) % PHI_SLOTS; };
-    auto th_slot = [&](int q) { return (q - z0 + 2 + 3 * TH_SLOTS) % TH_SLOTS; };
+    auto phi_slot = [&](int q) { return (q - z0 + 3 + 4 * PHI_SLOTS) % PHI_SLOTS; };
+    auto th_slot = [&](int q) { return (q - z0 + 2 + 4 * TH_SLOTS4) % TH_SLOTS4; };
 
-    // stage A: phi plane q into its ring slot (zero outside the box)
-    auto load_phi_plane = [&](int q) {
+    // phi plane q into its ring slot (zero outside the box); asynchronous or direct
+    auto load_phi_plane = [&](int q, bool async) {
         bool zok = true;
-        int wz = zwrap(q, zok);
+        const int wz = zwrap(q, zok);
         R* dst = phis + phi_slot(q) * R3N;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            int n = t + k * NT;
+            const int n = t + k * NT;
             if (n < R3N) {
-                R v = R(0);
-                if (zok && r3_ok[k]) v = CP::ld(p.pin, (long long)wz * plane + r3_off[k], p.inv_scale[F_PHI]);
-                dst[n] = v;
+                const bool ok = zok && r3_ok[k];
+                const long long g = (long long)wz * plane + r3_off[k];
+                if (async && ok) {
+                    cp_async<sizeof(SP)>(dst + n, p.pin + g);
+                } else {
+                    dst[n] = ok ? CP::ld(p.pin, g, R(1)) : R(0);
+                }
             }
         }
     };
-    // stage B: theta = phi(1-phi) n and g~ = n |g| on the R2 region of plane q
+    // moments (+ u_old) of plane q for the collision nodes of this thread
+    auto stage_plane = [&](int q) {
+        if constexpr (STG) {
+            bool zok = true;
+            const int wz = zwrap(q, zok);
+            if (!zok) return;
+            const long long zo = (long long)wz * plane;
+#pragma unroll 1
+            for (int k = 0; k < 2; ++k) {
+                const int node = k ? nodeB : nodeA;
+                const bool ok = k ? okB : okA;
+                if (node < 0 || !ok) continue;
+                const long long g = zo + (k ? offB : offA);
+#pragma unroll
+                for (int f = 0; f < 10; ++f) cp_async<sizeof(S)>(stg + f * R1N + node, p.min + f * N + g);
+                if (dr) {
+#pragma unroll
+                    for (int f = 0; f < 3; ++f) cp_async<sizeof(S)>(stg + (10 + f) * R1N + node, p.uin + f * N + g);
+                }
+            }
+        }
+    };
+    // theta = phi(1-phi) n on the theta region and g~ = n |g| on the collision
+    // region of plane q (compute_norm_interface, lb_cuda_auxfields_module.f90:72-119)
     auto theta_plane = [&](int q) {
         bool zok = true;
-        int wz = zwrap(q, zok);
+        const int wz = zwrap(q, zok);
         const R* f0 = phis + phi_slot(q - 1) * R3N;
         const R* f1 = phis + phi_slot(q) * R3N;
         const R* f2 = phis + phi_slot(q + 1) * R3N;
-        R* dst = ths + th_slot(q) * (TH_COMP * R2N);
+        R* th = ths + th_slot(q) * (3 * R2N);
+        R* gt = gts + th_slot(q) * (3 * R1N);
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            int n = t + k * NT;
+            const int n = t + k * NT;
             if (n >= R2N) continue;
-            int hx = n % R2X, hy = n / R2X;
-            int c3 = (hy + 1) * R3X + (hx + 1);
+            const int hx = n % R2X, hy = n / R2X;
+            const int c3 = (hy + 1) * R3X + (hx + 1);
             bool fluid = zok && r2_ok[k];
             if (fluid && obs) {
-                int s = p.isf[(long long)wz * plane + r2_off[k]];
+                const int s = p.isf[(long long)wz * plane + r2_off[k]];
                 fluid = (s == 1 || s == -1);
             }
             R th0 = 0, th1 = 0, th2 = 0, g0 = 0, g1 = 0, g2 = 0;
@@ -162,20 +228,23 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                 };
                 R gx, gy, gz;
                 iso_grad<R>(A, gx, gy, gz);
-                R mg = sqrt(gx * gx + gy * gy + gz * gz);
-                R den = mg + R(1.0e-9);
-                R nxv = gx / den, nyv = gy / den, nzv = gz / den;
-                R ph = f1[c3];
-                R pp = ph * (R(1) - ph);
+                const R mg = sqrt(gx * gx + gy * gy + gz * gz);
+                const R rden = rcp<R>(mg + R(1.0e-9));
+                const R nxv = gx * rden, nyv = gy * rden, nzv = gz * rden;
+                const R ph = f1[c3];
+                const R pp = ph * (R(1) - ph);
                 th0 = pp * nxv; th1 = pp * nyv; th2 = pp * nzv;
                 g0 = nxv * mg; g1 = nyv * mg; g2 = nzv * mg;
             }
-            dst[0 * R2N + n] = th0;
-            dst[1 * R2N + n] = th1;
-            dst[2 * R2N + n] = th2;
-            dst[3 * R2N + n] = g0;
-            dst[4 * R2N + n] = g1;
-            dst[5 * R2N + n] = g2;
+            th[0 * R2N + n] = th0;
+            th[1 * R2N + n] = th1;
+            th[2 * R2N + n] = th2;
+            if (hx >= 1 && hx <= R2X - 2 && hy >= 1 && hy <= R2Y - 2) {
+                const int n1 = (hy - 1) * R1X + (hx - 1);
+                gt[0 * R1N + n1] = g0;
+                gt[1 * R1N + n1] = g1;
+                gt[2 * R1N + n1] = g2;
+            }
         }
     };
 
@@ -185,53 +254,61 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
 #pragma unroll
     for (int i = 0; i < 10; ++i) am[i] = a0[i] = ap[i] = R(0);
 
+    // ---- prologue: phi(z0-3..z0+2), theta(z0-2..z0), staged moments of plane z0-1 ----
     if constexpr (TC) {
-        for (int q = z0 - 3; q <= z0 + 1; ++q) load_phi_plane(q);
+        for (int q = z0 - 3; q <= z0 + 1; ++q) load_phi_plane(q, false);
         __syncthreads();
         theta_plane(z0 - 2);
         theta_plane(z0 - 1);
         __syncthreads();
+        theta_plane(z0);               // reads phi(z0-1..z0+1)
+        load_phi_plane(z0 + 2, true);  // into the slot of phi(z0-3), no longer read
     }
+    stage_plane(z0 - 1);
+    cp_async_wait_all();
+    __syncthreads();
 
     for (int q = z0 - 1; q <= z1; ++q) {
-        if constexpr (TC) {
-            // A: prefetch phi(q+3) into the slot of phi(q-2) (last read by stage C of
-            //    the previous iteration, which ended with a barrier).
-            // B: theta(q+1) from phi(q..q+2) into the slot of theta(q-2).
-            load_phi_plane(q + 3);
-            theta_plane(q + 1);
-            __syncthreads();
-        }
         bool zok = true;
         const int wz = zwrap(q, zok);
         const long long zoff = (long long)wz * plane;
         const bool q_inner = (q >= z0) && (q < z1);
 
-        // ---------------- stage C: prologue + collision on the R1 region ----------------
-        for (int pass = 0; pass < 2; ++pass) {
-            const int node = pass ? r1n1 : r1n0;
-            if (node < 0) break;
-            const bool inb = zok && (pass ? r1ok1 : r1ok0);
-            const long long gi = zoff + (pass ? r1off1 : r1off0);
+        // ================= phase 1 =================
+        // theta(q+2) reads phi(q+1..q+3) and replaces theta(q-2)
+        if constexpr (TC) theta_plane(q + 2);
+
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            const int node = k ? nodeB : nodeA;
+            if (node < 0) continue;
+            const bool inb = zok && (k ? okB : okA);
+            const long long gi = zoff + (k ? offB : offA);
             int isf = 1;
             if (inb && obs) isf = p.isf[gi];
+            const bool live = inb && (isf != 0);
+            const bool interior = (k == 0) && out_ok && q_inner;
             R fpop[27];
-            bool live = inb && (isf != 0);
-            NodeState<R> st;
-            R phi_new = 0;
-            bool interior = (pass == 0) && out_ok && q_inner;
+            R sP = 0, spxx = 0, spyy = 0, spzz = 0, spxy = 0, spxz = 0, spyz = 0, som = 0;
             if (live) {
-                // input moments
-                R P = CD::ld(p.min, 0 * N + gi, p.inv_scale[0]);
-                R u = CD::ld(p.min, 1 * N + gi, p.inv_scale[1]);
-                R v = CD::ld(p.min, 2 * N + gi, p.inv_scale[2]);
-                R w = CD::ld(p.min, 3 * N + gi, p.inv_scale[3]);
-                R pxx = CD::ld(p.min, 4 * N + gi, p.inv_scale[4]);
-                R pyy = CD::ld(p.min, 5 * N + gi, p.inv_scale[5]);
-                R pzz = CD::ld(p.min, 6 * N + gi, p.inv_scale[6]);
-                R pxy = CD::ld(p.min, 7 * N + gi, p.inv_scale[7]);
-                R pxz = CD::ld(p.min, 8 * N + gi, p.inv_scale[8]);
-                R pyz = CD::ld(p.min, 9 * N + gi, p.inv_scale[9]);
+                R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;
+                if constexpr (STG) {
+                    P = (R)stg[0 * R1N + node]; u = (R)stg[1 * R1N + node];
+                    v = (R)stg[2 * R1N + node]; w = (R)stg[3 * R1N + node];
+                    pxx = (R)stg[4 * R1N + node]; pyy = (R)stg[5 * R1N + node]; pzz = (R)stg[6 * R1N + node];
+                    pxy = (R)stg[7 * R1N + node]; pxz = (R)stg[8 * R1N + node]; pyz = (R)stg[9 * R1N + node];
+                } else {
+                    P = CD::ld(p.min, 0 * N + gi, p.inv_scale[0]);
+                    u = CD::ld(p.min, 1 * N + gi, p.inv_scale[1]);
+                    v = CD::ld(p.min, 2 * N + gi, p.inv_scale[2]);
+                    w = CD::ld(p.min, 3 * N + gi, p.inv_scale[3]);
+                    pxx = CD::ld(p.min, 4 * N + gi, p.inv_scale[4]);
+                    pyy = CD::ld(p.min, 5 * N + gi, p.inv_scale[5]);
+                    pzz = CD::ld(p.min, 6 * N + gi, p.inv_scale[6]);
+                    pxy = CD::ld(p.min, 7 * N + gi, p.inv_scale[7]);
+                    pxz = CD::ld(p.min, 8 * N + gi, p.inv_scale[8]);
+                    pyz = CD::ld(p.min, 9 * N + gi, p.inv_scale[9]);
+                }
                 R phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
                 if constexpr (TC) {
                     const int hx = node % R1X, hy = node / R1X;
@@ -246,9 +323,9 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                     };
                     phi = f1[c3];
                     lap = iso_lap<R>(A);
-                    const R* t0 = ths + th_slot(q - 1) * (TH_COMP * R2N);
-                    const R* t1 = ths + th_slot(q) * (TH_COMP * R2N);
-                    const R* t2 = ths + th_slot(q + 1) * (TH_COMP * R2N);
+                    const R* t0 = ths + th_slot(q - 1) * (3 * R2N);
+                    const R* t1 = ths + th_slot(q) * (3 * R2N);
+                    const R* t2 = ths + th_slot(q + 1) * (3 * R2N);
                     auto TXa = [&](int a, int b, int c) -> R {
                         const R* f = c < 0 ? t0 : (c > 0 ? t2 : t1);
                         return f[0 * R2N + c2 + b * R2X + a];
@@ -262,23 +339,24 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                         return f[2 * R2N + c2 + b * R2X + a];
                     };
                     divt = iso_div<R>(TXa, TYa, TZa);
-                    gfx = t1[3 * R2N + c2];
-                    gfy = t1[4 * R2N + c2];
-                    gfz = t1[5 * R2N + c2];
+                    const R* g1 = gts + th_slot(q) * (3 * R1N);
+                    gfx = g1[0 * R1N + node];
+                    gfy = g1[1 * R1N + node];
+                    gfz = g1[2 * R1N + node];
                 }
                 // ---- moments prologue: lb_cuda_moments_module.f90:104-339 ----
-                R rhophi = R(1), inv = R(1), mask = R(0), fxv, fyv, fzv;
+                R inv = R(1), mask = R(0), fxv, fyv, fzv;
                 if constexpr (TC) mask = R(4) * phi * (R(1) - phi);
                 if (dr) {
-                    rhophi = p.rho_r * phi + (R(1) - phi) * p.rho_b;
-                    inv = R(1) / rhophi;
+                    const R rhophi = p.rho_r * phi + (R(1) - phi) * p.rho_b;
+                    inv = rcp<R>(rhophi);
                     fxv = rhophi * p.fx; fyv = rhophi * p.fy; fzv = rhophi * p.fz;
                 } else {
                     fxv = p.fx; fyv = p.fy; fzv = p.fz;
                 }
                 R grx = 0, gry = 0, grz = 0, cv = 0, omega;
                 if constexpr (TC) {
-                    R chem = R(4) * p.beta * phi * (phi - R(1)) * (phi - R(0.5)) - p.kapp * lap;
+                    const R chem = R(4) * p.beta * phi * (phi - R(1)) * (phi - R(0.5)) - p.kapp * lap;
                     fxv += chem * gfx;
                     fyv += chem * gfy;
                     fzv += chem * gfz;
@@ -286,29 +364,34 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                 if (dr) {
                     const R drho = p.rho_r - p.rho_b;
                     grx = drho * gfx; gry = drho * gfy; grz = drho * gfz;
-                    R mp = mask * P * cssq;
+                    const R mp = mask * P * cssq;
                     fxv -= mp * grx; fyv -= mp * gry; fzv -= mp * grz;
                 }
                 R tfx = fxv, tfy = fyv, tfz = fzv;
                 if (dr) {
-                    R uo = CD::ld(p.uin, 0 * N + gi, p.inv_scale[F_UOLD + 0]);
-                    R vo = CD::ld(p.uin, 1 * N + gi, p.inv_scale[F_UOLD + 1]);
-                    R wo = CD::ld(p.uin, 2 * N + gi, p.inv_scale[F_UOLD + 2]);
-                    R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
-                    R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
-                    R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
-                    R tau = visc * R(3) + R(0.5);
-                    omega = R(1) / tau;
-                    cv = mask * visc / (tau * cssq);
+                    R uo, vo, wo;
+                    if constexpr (STG) {
+                        uo = (R)stg[10 * R1N + node]; vo = (R)stg[11 * R1N + node]; wo = (R)stg[12 * R1N + node];
+                    } else {
+                        uo = CD::ld(p.uin, 0 * N + gi, p.inv_scale[F_UOLD + 0]);
+                        vo = CD::ld(p.uin, 1 * N + gi, p.inv_scale[F_UOLD + 1]);
+                        wo = CD::ld(p.uin, 2 * N + gi, p.inv_scale[F_UOLD + 2]);
+                    }
+                    const R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
+                    const R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
+                    const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
+                    omega = rcp<R>(visc * R(3) + R(0.5));
+                    // mask * visc / (tau cs^2), with 1/tau = omega
+                    cv = mask * visc * omega * R(3);
                     fxv -= cv * (qxx * grx + qxy * gry + qxz * grz);
                     fyv -= cv * (qyy * gry + qxy * grx + qyz * grz);
                     fzv -= cv * (qzz * grz + qxz * grx + qyz * gry);
-                    R tmp = -p.sharp_c * divt;
+                    const R tmp = -p.sharp_c * divt;
                     u += R(0.5) * fxv * inv;
                     v += R(0.5) * fyv * inv;
                     w += R(0.5) * fzv * inv;
-                    R dd = (p.rho_r - p.rho_b) * (p.tau_diff * lap + tmp);
-                    R den = R(1) / (R(1) - R(0.5) * dd * inv);
+                    const R dd = (p.rho_r - p.rho_b) * (p.tau_diff * lap + tmp);
+                    const R den = rcp<R>(R(1) - R(0.5) * dd * inv);
                     u *= den; v *= den; w *= den;
                     tfx -= dd * u; tfy -= dd * v; tfz -= dd * w;
                     fxv -= dd * u; fyv -= dd * v; fzv -= dd * w;
@@ -317,8 +400,8 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                     v += R(0.5) * fyv * inv;
                     w += R(0.5) * fzv * inv;
                     if constexpr (TC) {
-                        R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
-                        omega = R(1) / (visc * R(3) + R(0.5));
+                        const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
+                        omega = rcp<R>(visc * R(3) + R(0.5));
                     } else {
                         omega = p.omega;
                     }
@@ -330,8 +413,8 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                 pxz += R(0.5) * (fzv * u + fxv * w) * inv;
                 pyz += R(0.5) * (fzv * v + fyv * w) * inv;
                 if (dr) {
-                    R qxx = pxx - u * u, qyy = pyy - v * v, qzz = pzz - w * w;
-                    R qxy = pxy - u * v, qxz = pxz - u * w, qyz = pyz - v * w;
+                    const R qxx = pxx - u * u, qyy = pyy - v * v, qzz = pzz - w * w;
+                    const R qxy = pxy - u * v, qxz = pxz - u * w, qyz = pyz - v * w;
                     tfx -= cv * (qxx * grx + qxy * gry + qxz * grz);
                     tfy -= cv * (qyy * gry + qxy * grx + qyz * grz);
                     tfz -= cv * (qzz * grz + qxz * grx + qyz * gry);
@@ -345,83 +428,74 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                     }
                     if constexpr (TC) {
                         // update_phifields: lb_cuda_update_phi_module.f90:77-93
-                        phi_new = phi - u * R(0.5) * gfx - v * R(0.5) * gfy - w * R(0.5) * gfz + p.tau_diff * lap -
-                                  p.sharp_c * divt;
+                        const R phi_new = phi - u * R(0.5) * gfx - v * R(0.5) * gfy - w * R(0.5) * gfz +
+                                          p.tau_diff * lap - p.sharp_c * divt;
                         CP::st(p.pout, gi, phi_new, p.scale[F_PHI]);
                     }
                 }
                 // ---- collision: lb_cuda_fused_module.f90:531-713 ----
-                st.P = P;
-                st.u = u; st.v = v; st.w = w;
-                st.pxx = pxx - u * u; st.pyy = pyy - v * v; st.pzz = pzz - w * w;
-                st.pxy = pxy - u * v; st.pxz = pxz - u * w; st.pyz = pyz - v * w;
-                st.Fx = tfx * inv; st.Fy = tfy * inv; st.Fz = tfz * inv;
-                st.omega = omega;
+                const R Xn = pxx - u * u, Yn = pyy - v * v, Zn = pzz - w * w;
+                const R XYn = pxy - u * v, XZn = pxz - u * w, YZn = pyz - v * w;
+                const R Fx = tfx * inv, Fy = tfy * inv, Fz = tfz * inv;
+                sP = P;
+                spxx = Xn; spyy = Yn; spzz = Zn; spxy = XYn; spxz = XZn; spyz = YZn; som = omega;
                 const R om1 = R(1) - omega;
-                // Hermite coefficients up to second order
                 const R m0 = P;
-                const R mx = u + R(0.5) * st.Fx, my = v + R(0.5) * st.Fy, mz = w + R(0.5) * st.Fz;
-                const R mxx = u * u + om1 * st.pxx + u * st.Fx;
-                const R myy = v * v + om1 * st.pyy + v * st.Fy;
-                const R mzz = w * w + om1 * st.pzz + w * st.Fz;
-                const R mxy = u * v + om1 * st.pxy + R(0.5) * (u * st.Fy + v * st.Fx);
-                const R mxz = u * w + om1 * st.pxz + R(0.5) * (u * st.Fz + w * st.Fx);
-                const R myz = v * w + om1 * st.pyz + R(0.5) * (v * st.Fz + w * st.Fy);
+                const R mx = u + R(0.5) * Fx, my = v + R(0.5) * Fy, mz = w + R(0.5) * Fz;
+                const R mxx = u * u + om1 * Xn + u * Fx;
+                const R myy = v * v + om1 * Yn + v * Fy;
+                const R mzz = w * w + om1 * Zn + w * Fz;
+                const R mxy = u * v + om1 * XYn + R(0.5) * (u * Fy + v * Fx);
+                const R mxz = u * w + om1 * XZn + R(0.5) * (u * Fz + w * Fx);
+                const R myz = v * w + om1 * YZn + R(0.5) * (v * Fz + w * Fy);
                 if constexpr (LAT == 27) {
-                    // M[a][b][c]: coefficient with x/y/z multiplicities a, b, c
                     R M[3][3][3];
                     M[0][0][0] = m0;
                     M[1][0][0] = mx; M[0][1][0] = my; M[0][0][1] = mz;
                     M[2][0][0] = mxx; M[0][2][0] = myy; M[0][0][2] = mzz;
                     M[1][1][0] = mxy; M[1][0][1] = mxz; M[0][1][1] = myz;
                     if constexpr (HO) {
-                        const R X = st.pxx, Y = st.pyy, Z = st.pzz, XY = st.pxy, XZ = st.pxz, YZ = st.pyz;
+                        const R X = Xn, Y = Yn, Z = Zn, XY = XYn, XZ = XZn, YZ = YZn;
                         const R u2 = u * u, v2 = v * v, w2 = w * w;
-                        // recursive non-equilibrium terms, rows 10..26 (lb_cuda_fused_module.f90:686-703)
-                        M[2][1][0] = u2 * v + om1 * (R(2) * XY * u + X * v);                          // 10 xxy
-                        M[2][0][1] = u2 * w + om1 * (R(2) * XZ * u + X * w);                          // 11 xxz
-                        M[1][2][0] = u * v2 + om1 * (Y * u + R(2) * XY * v);                          // 12 xyy
-                        M[1][0][2] = u * w2 + om1 * (Z * u + R(2) * XZ * w);                          // 13 xzz
-                        M[0][1][2] = v * w2 + om1 * (Z * v + R(2) * YZ * w);                          // 14 yzz
-                        M[0][2][1] = v2 * w + om1 * (R(2) * YZ * v + Y * w);                          // 15 yyz
-                        M[1][1][1] = u * v * w + om1 * (YZ * u + XZ * v + XY * w);                    // 16 xyz
-                        M[2][2][0] = u2 * v2 + om1 * (Y * u2 + R(2) * v * (R(3) * XY * u + X * v));   // 17
-                        M[2][0][2] = u2 * w2 + om1 * (Z * u2 + R(2) * w * (R(3) * XZ * u + X * w));   // 18
-                        M[0][2][2] = v2 * w2 + om1 * (Z * v2 + R(2) * w * (R(3) * YZ * v + Y * w));   // 19
-                        M[1][1][2] = u * v * w2 +
-                                     om1 * (Z * u * v + w * (R(3) * YZ * u + R(3) * XZ * v + R(2) * XY * w));  // 20
+                        // rows 10..26 of the reference (lb_cuda_fused_module.f90:667-703)
+                        M[2][1][0] = u2 * v + om1 * (R(2) * XY * u + X * v);
+                        M[2][0][1] = u2 * w + om1 * (R(2) * XZ * u + X * w);
+                        M[1][2][0] = u * v2 + om1 * (Y * u + R(2) * XY * v);
+                        M[1][0][2] = u * w2 + om1 * (Z * u + R(2) * XZ * w);
+                        M[0][1][2] = v * w2 + om1 * (Z * v + R(2) * YZ * w);
+                        M[0][2][1] = v2 * w + om1 * (R(2) * YZ * v + Y * w);
+                        M[1][1][1] = u * v * w + om1 * (YZ * u + XZ * v + XY * w);
+                        M[2][2][0] = u2 * v2 + om1 * (Y * u2 + R(2) * v * (R(3) * XY * u + X * v));
+                        M[2][0][2] = u2 * w2 + om1 * (Z * u2 + R(2) * w * (R(3) * XZ * u + X * w));
+                        M[0][2][2] = v2 * w2 + om1 * (Z * v2 + R(2) * w * (R(3) * YZ * v + Y * w));
+                        M[1][1][2] = u * v * w2 + om1 * (Z * u * v + w * (R(3) * YZ * u + R(3) * XZ * v + R(2) * XY * w));
                         M[1][2][1] = u * v2 * w +
-                                     om1 * (R(2) * YZ * u * v + XZ * v2 + R(2) * Y * u * w + R(4) * XY * v * w);  // 21
+                                     om1 * (R(2) * YZ * u * v + XZ * v2 + R(2) * Y * u * w + R(4) * XY * v * w);
                         M[2][1][1] = u2 * v * w +
-                                     om1 * (YZ * u2 + R(2) * XZ * u * v + R(4) * XY * u * w + R(2) * X * v * w);  // 22
-                        M[2][1][2] = u2 * v * w2 +
-                                     om1 * (Z * u2 * v + R(3) * w * (YZ * u2 + R(2) * XZ * u * v + R(2) * XY * u * w +
-                                                                     X * v * w));  // 23
+                                     om1 * (YZ * u2 + R(2) * XZ * u * v + R(4) * XY * u * w + R(2) * X * v * w);
+                        M[2][1][2] = u2 * v * w2 + om1 * (Z * u2 * v + R(3) * w * (YZ * u2 + R(2) * XZ * u * v +
+                                                                                 R(2) * XY * u * w + X * v * w));
                         M[2][2][1] = u2 * v2 * w + om1 * (R(2) * u * v * (YZ * u + XZ * v) + R(2) * Y * u2 * w +
-                                                          v * (R(10) * XY * u + R(3) * X * v) * w);  // 24
-                        M[1][2][2] = u * v2 * w2 +
-                                     om1 * (Z * u * v2 + R(3) * w * (R(2) * YZ * u * v + XZ * v2 + Y * u * w +
-                                                                     R(2) * XY * v * w));  // 25
+                                                          v * (R(10) * XY * u + R(3) * X * v) * w);
+                        M[1][2][2] = u * v2 * w2 + om1 * (Z * u * v2 + R(3) * w * (R(2) * YZ * u * v + XZ * v2 +
+                                                                                  Y * u * w + R(2) * XY * v * w));
                         M[2][2][2] = u2 * v2 * w2 +
                                      om1 * (Z * u2 * v2 + w * (R(6) * u * v * (YZ * u + XZ * v) + R(3) * Y * u2 * w +
-                                                               R(2) * v * (R(7) * XY * u + R(2) * X * v) * w));  // 26
+                                                               R(2) * v * (R(7) * XY * u + R(2) * X * v) * w));
                     } else {
                         M[2][1][0] = M[2][0][1] = M[1][2][0] = M[1][0][2] = M[0][1][2] = M[0][2][1] = M[1][1][1] = R(0);
                         M[2][2][0] = M[2][0][2] = M[0][2][2] = M[1][1][2] = M[1][2][1] = M[2][1][1] = R(0);
                         M[2][1][2] = M[2][2][1] = M[1][2][2] = M[2][2][2] = R(0);
                     }
-                    // x pass: T[cx][b][c]
                     R T[3][3][3];
 #pragma unroll
                     for (int b = 0; b < 3; ++b)
 #pragma unroll
                         for (int c = 0; c < 3; ++c) d1q3_inv<R>(M[0][b][c], M[1][b][c], M[2][b][c], T[0][b][c], T[1][b][c], T[2][b][c]);
-                    // y pass: U[cx][cy][c] (reuse M)
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
 #pragma unroll
                         for (int c = 0; c < 3; ++c) d1q3_inv<R>(T[a][0][c], T[a][1][c], T[a][2][c], M[a][0][c], M[a][1][c], M[a][2][c]);
-                    // z pass: populations
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -433,7 +507,6 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
                             fpop[LINK(a - 1, b - 1, 1)] = vp;
                         }
                 } else {
-                    // D3Q19: f*_l = w_l [m0 + 3 c.m1 + 4.5 H2(c):m2]
                     const R base = m0 - R(1.5) * (mxx + myy + mzz);
 #pragma unroll
                     for (int l = 0; l < 19; ++l) {
@@ -454,24 +527,22 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
 
             // ---- obstacle bounce-back: lb_cuda_boundary_module.f90:162-199 ----
             if (interior && obs && isf == -1) {
-                const R om1 = R(1) - st.omega;
+                const R om1 = R(1) - som;
 #pragma unroll
                 for (int l = 1; l < LAT; ++l) {
                     const int cx = EX(l), cy = EY(l), cz = EZ(l);
-                    // upstream node x - c_l
                     const int ix = 1 - cx, iy = 1 - cy;
-                    bool ok = nbx_ok[ix] && nby_ok[iy];
                     bool zk = true;
-                    int zz = zwrap(q - cz, zk);
+                    const int zz = zwrap(q - cz, zk);
                     int s = 1;
-                    if (ok && zk) s = p.isf[(long long)zz * plane + (long long)nby[iy] * nx + nbx[ix]];
+                    if (nbx_ok[ix] && nby_ok[iy] && zk) s = p.isf[(long long)zz * plane + (long long)nby[iy] * nx + nbx[ix]];
                     if (s != 0) continue;
                     const R wl = R(WL<LAT>(l));
                     const R dx = R(cx), dy = R(cy), dz = R(cz);
-                    R fneq = wl * R(4.5) *
-                             ((dx * dx - cssq) * st.pxx + (dy * dy - cssq) * st.pyy + (dz * dz - cssq) * st.pzz +
-                              R(2) * (dx * dy) * st.pxy + R(2) * (dx * dz) * st.pxz + R(2) * (dy * dz) * st.pyz);
-                    R fp = wl * st.P + om1 * fneq;
+                    const R fneq = wl * R(4.5) *
+                                   ((dx * dx - cssq) * spxx + (dy * dy - cssq) * spyy + (dz * dz - cssq) * spzz +
+                                    R(2) * (dx * dy) * spxy + R(2) * (dx * dz) * spxz + R(2) * (dy * dz) * spyz);
+                    const R fp = wl * sP + om1 * fneq;
                     a0[0] += fp;
                     a0[1] += fp * dx; a0[2] += fp * dy; a0[3] += fp * dz;
                     a0[4] += fp * (dx * dx); a0[5] += fp * (dy * dy); a0[6] += fp * (dz * dz);
@@ -481,11 +552,14 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
         }
         __syncthreads();
 
-        // ---------------- stage D: pull populations of plane q ----------------
+        // ================= phase 2 =================
+        // the staging area and the slot of phi(q-1) were last read in phase 1
+        if (q < z1) stage_plane(q + 1);
+        if constexpr (TC) load_phi_plane(q + 4, true);
+
 #pragma unroll
         for (int zc = 0; zc < 3; ++zc) {
             const int cz = zc - 1;
-            // x sums for each cy
             R S0[3], S1[3], S2[3];
 #pragma unroll
             for (int yc = 0; yc < 3; ++yc) {
@@ -535,7 +609,8 @@ __global__ void __launch_bounds__(NT, 2) stream_kernel(const StepParams<S, R> p)
             a0[i] = ap[i];
             ap[i] = R(0);
         }
-        if constexpr (!TC) __syncthreads();
+        cp_async_wait_all();
+        __syncthreads();
     }
 }
 
