@@ -43,6 +43,10 @@ METRIC = "MLUPS (D3Q27 high-order two-component lattice updates per second)"
 UNIT = "MLUPS"
 LBOX = 256
 B_LUP = {"f32": 112, "f16": 60, "bf16": 60, "f64": 224}  # algorithmic bytes per lattice update
+# DRAM bytes (read + write) of one step launch from one ncu capture at this
+# workload: profiles/stream_kernel_laplace256_f32.md and
+# profiles/stream_kernel_laplace256_full.md
+NCU_TRAFFIC = {("f32", 256): 1886000000}
 
 
 def workload(storage: str = "f32", L: int = LBOX):
@@ -80,7 +84,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -239,7 +243,7 @@ def cpu_baseline(storage: str, L: int, nsteps: int, threads: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
@@ -288,13 +292,7 @@ def main():
                          f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
     if rank != 0:
         return
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = _json.load(open(tpath)).get(f"{args.storage}_{args.box}")
-        except (OSError, ValueError):
-            traffic = None
+    traffic = NCU_TRAFFIC.get((args.storage, args.box))
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_step"], "higher_is_better": True, "scaling": "weak",
