@@ -132,6 +132,28 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press);
  * (mpi_module.f90:7491-7560) on one rank.  out[5] = {phi, P, u, v, w}. */
 int lbf_reduce(lbf_handle* h, double out[5]);
 
+/* ---- allocation-free reduction ----
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory while they run: a Fortran integrator whose device
+ * arrays belong to OpenACC data regions and reach the library only as device
+ * pointers, a time loop captured into a CUDA graph (cudaMalloc cannot be
+ * captured and synchronises the device), a solver held to a fixed device
+ * memory budget.  Computes the same FP64 sums as lbf_reduce -- phi, P, u, v,
+ * w over nodes with isfluid = 1 or -1 -- over caller-owned device arrays:
+ * mom10 (float, 10 x lx*ly*lz, only the first four fields are read), phi
+ * (float, may be NULL), isfluid (int8, may be NULL = all fluid).  out is a
+ * host array of 5 doubles.  It calls no cudaMalloc/cudaFree: its scratch is a
+ * file-scope __device__ array of LBF_NOALLOC_MAX_PLANES + 1 rows of five
+ * doubles (328 KB held on every GPU that loads the library until process
+ * exit); boxes with lz > LBF_NOALLOC_MAX_PLANES are rejected with LBF_E_ARG.
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race.  Runs on the legacy
+ * default stream and returns after the totals reached `out`. */
+#define LBF_NOALLOC_MAX_PLANES 8192
+int lbf_reduce_noalloc(const float* mom10, const float* phi, const int8_t* isfluid, int lx, int ly, int lz,
+                       double out[5]);
+
 /* ---- host-side set-up helpers (the driver's part of LBFAST.f90) ---- */
 
 /* LBFAST.f90:258-325: from raw isfluid (1 fluid / 0 solid, as read from

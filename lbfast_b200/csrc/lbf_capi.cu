@@ -47,6 +47,10 @@ const int EZh[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -
 
 }  // namespace
 
+namespace lbf {
+void record_error(const char* msg) { g_last_error = msg; }
+}  // namespace lbf
+
 struct lbf_handle {
     lbf_params p;
     int nx = 0, ny = 0, nz = 0;

@@ -79,6 +79,9 @@ cudaError_t launch_reduce(int storage, long long N, const void* mom, const void*
                           const double* inv_scale, double* d_out, cudaStream_t st);
 
 size_t storage_bytes(int storage);
+
+// sets the message returned by lbf_last_error on the calling thread
+void record_error(const char* msg);
 size_t phi_bytes(int storage);
 
 }  // namespace lbf
