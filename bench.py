@@ -3,9 +3,11 @@
 Workload (the reference's Laplace check, the configuration its headline
 metric is quoted on that fits one GPU): two-component DENSRATIO D3Q27
 HIGHORDER, 256^3 periodic, FP32, a centred droplet R=40 with the
-fcut_tanh profile of width 3, density ratio 100 (rho_r = 1, rho_b = 0.01),
-sigma = 0.03, nu1 = nu2 = 0.1, tau_diff = 0.1, fluids at rest.  Synthetic
-input generated in-process (no dataset exists for this path).
+fcut_tanh profile of width 3, density ratio 100 (rho_r = 100 in the droplet,
+rho_b = 1 around it), sigma = 0.03, nu1 = nu2 = 0.1, tau_diff = 0.1, fluids at
+rest.  Synthetic input generated in-process (no dataset exists for this
+path).  The same ratio written as rho_r = 1, rho_b = 0.01 makes the scheme
+unstable after ~3000 steps at this size, in FP64 as in FP32.
 
 One "step" is one LB time step of the whole box.  The timed region covers
 exactly --steps steps between barriers and device synchronisations, timed with
@@ -42,7 +44,8 @@ sys.path.insert(0, ROOT)
 METRIC = "MLUPS (D3Q27 high-order two-component lattice updates per second)"
 UNIT = "MLUPS"
 LBOX = 256
-B_LUP = {"f32": 112, "f16": 60, "bf16": 60, "f64": 224}  # algorithmic bytes per lattice update
+RHO_R, RHO_B = 100.0, 1.0
+B_LUP = {"f32": 112, "f16": 64, "bf16": 64, "f64": 224}  # algorithmic bytes per lattice update
 # DRAM bytes (read + write) of one step launch from one ncu capture at this
 # workload: profiles/stream_kernel_laplace256_f32.md and
 # profiles/stream_kernel_laplace256_full.md
@@ -52,15 +55,16 @@ NCU_TRAFFIC = {("f32", 256): 1886000000}
 def workload(storage: str = "f32", L: int = LBOX):
     import lbfast_b200 as lbf
     p = lbf.Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1,
-                   visc1=0.1, visc2=0.1, rho_r=1.0, rho_b=0.01, sigma=0.03, width=3.0, tau_diff=0.1,
+                   visc1=0.1, visc2=0.1, rho_r=RHO_R, rho_b=RHO_B, sigma=0.03, width=3.0, tau_diff=0.1,
                    printphi=1, storage=storage)
     R = 40.0 * L / 256
-    m, phi = lbf.ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, 1.0, 0.01, True)
+    m, phi = lbf.ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, RHO_R, RHO_B, True)
     return p, m, phi
 
 
 def config_dict(storage, L=LBOX):
-    return {"workload": f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO (100:1), "
+    return {"workload": f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO "
+                        f"(rho_r/rho_b = {RHO_R:g}/{RHO_B:g}), "
                         f"R={int(40 * L / 256)}, width 3, sigma 0.03",
             "box": [L, L, L], "lattice": "D3Q27", "highorder": True, "twocomponent": True, "densratio": True,
             "storage": storage, "bytes_per_lup": B_LUP[storage],
@@ -119,33 +123,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_init():
-    import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
-    return rank, local, world
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def allmax(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+from lbfast_b200.replicas import allmax, barrier, init_from_env, shutdown, weak_scaling_value  # noqa: E402
 
 
 def run_ours(args, rank, local, world):
@@ -175,7 +153,7 @@ def run_ours(args, rank, local, world):
     ms = allmax(e0.elapsed_time(e1), world)
     clocks = clk.summary()
     ms_step = ms / args.steps
-    value = world * N * args.steps / (ms * 1e-3) / 1e6
+    value = weak_scaling_value(N, args.steps, ms, world)
     # the step kernel is the only launch per step: its average duration is the step time
     bytes_launch = B_LUP[args.storage] * N
     achieved = bytes_launch / (ms_step * 1e-3) / 1e9
@@ -215,7 +193,7 @@ def run_ours(args, rank, local, world):
     s.close()
     h2d = (10 + 1) * N * 4
     d2h = 5 * N * 4
-    e2e = {"value": world * N * args.steps / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+    e2e = {"value": weak_scaling_value(N, args.steps, ms_e2e, world), "unit": UNIT,
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
            "path": "lbf_set_fields (pinned host, f32) + lbf_step + lbf_get_print_fields; the initial state is "
                    "uploaded once and copy_print read back once per run, the reference's stamp = nsteps cadence"}
@@ -253,11 +231,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    rank, local, world = dist_init()
+    rank, local, world = init_from_env()
     threads = os.cpu_count() or 1
 
     if args.impl == "reference":
         if rank != 0:
+            shutdown(world)
             return
         # each timed step of the reference arm is one full oracle step of the box
         for _ in range(min(args.warmup, 1)):
@@ -273,6 +252,7 @@ def main():
                                            f"reference kernels (oracle/lbf_oracle.c), OpenMP over z"},
                 "e2e": {"value": mlups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        shutdown(world)
         return
 
     import json as _json
@@ -291,6 +271,7 @@ def main():
                "sample": f"{args.cpu_steps} steps of the same {args.box}^3 box ({dt:.1f} s), FP32 C restatement of "
                          f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
     if rank != 0:
+        shutdown(world)
         return
     traffic = NCU_TRAFFIC.get((args.storage, args.box))
     line = {
@@ -305,9 +286,7 @@ def main():
         "finite": r["finite"],
     }
     print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    shutdown(world)
 
 
 if __name__ == "__main__":

@@ -64,7 +64,9 @@ typedef struct lbf_params {
     double sigma, width;     /* surface tension, interface width */
     double tau_diff;         /* phase-field diffusivity */
     double fx, fy, fz;       /* body force */
-    double wettab_r;         /* contact angle in degrees (obstacles, two components) */
+    double wettab_r;         /* contact angle in degrees (obstacles, two components); the reference
+                                applies it only with WETTABILITY and otherwise uses 90
+                                (lb_cuda_boundary_module.f90:264,275) */
     int printphi;            /* PRINTPHI: `rho` output holds phi */
     int zseg;                /* planes per z segment of the kernel; 0 = automatic */
 } lbf_params;
@@ -173,6 +175,31 @@ int lbf_ic_taylor_green(int lx, int ly, int lz, double u0, double* mom10);
  * branch, init_conditions_module.f90:394-426): phi and mom10 on fluid nodes. */
 int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
                    double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* mom10, double* phi);
+
+/* LAMBTEST initial droplet (init_conditions_module.f90:355-393): as
+ * lbf_ic_droplet with the x distance halved (an ellipsoid twice as long in x). */
+int lbf_ic_lamb(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
+                double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* mom10, double* phi);
+
+/* Run controls of the `simulation` and `fluid` namelists that are not
+ * lbf_params (LBFAST.f90:32-60), with the DOBENCHMARK defaults of
+ * LBFAST.f90:159-191. */
+typedef struct lbf_run {
+    int nsteps, stamp, stamp2D, stamp_term, stepskip;
+    int lreadisfluid, lreadinit, lprint, lvtk, lraw, lrestart, lwriterestart;
+    int openbc, nplanes, every_time_check;
+    int iprobe, jprobe, kprobe;
+    double time_limit;
+    double uwall, radius, width, center[3];
+} lbf_run;
+
+/* Reads the `simulation` and `fluid` namelists of a reference input file
+ * (LBFAST.f90:193-232) into p (physics) and run (controls); p->lx..wettab_r
+ * and run are first set to the DOBENCHMARK defaults.  The compile-time macro
+ * fields of p (lattice, highorder, twocomponent, densratio, obstacles,
+ * storage, printphi) are left as the caller set them.  Unknown keys,
+ * malformed values, openbc = 1 and lrestart = .true. are errors. */
+int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run);
 
 /* raw + XDMF writer of print_raw_sync (print_module.f90:2007-2180): writes
  * <dir>/out_rho_NNNNNN.raw/.xdmf, out_vel_..., and out_press_... when press

@@ -63,6 +63,7 @@ struct lbf_handle {
     void* mom[2] = {nullptr, nullptr};
     void* uold[2] = {nullptr, nullptr};
     void* phi[2] = {nullptr, nullptr};
+    float* pres[2] = {nullptr, nullptr};  // P in FP32 when the other moments are 16-bit
     int8_t* isf = nullptr;
     bool isf_set = false;
     int cur = 0;
@@ -107,6 +108,7 @@ void free_all(lbf_handle* h) {
         cudaFree(h->mom[b]);
         cudaFree(h->uold[b]);
         cudaFree(h->phi[b]);
+        cudaFree(h->pres[b]);
         cudaFree(h->wetW[b]);
     }
     cudaFree(h->isf);
@@ -187,14 +189,19 @@ int prime(lbf_handle* h) {
     return LBF_OK;
 }
 
-// per-field storage scale for 16-bit storage: the largest magnitude maps into
-// [2^11, 2^12), leaving a factor 16 of headroom below the FP16 maximum
-double pick_scale(int storage, double maxabs, double fallback) {
+// power-of-two storage scale of a 16-bit field group: FP16 carries an 11-bit
+// significand over 30 binades (6.1e-5 .. 65504), so the scale only has to keep
+// values in range; the largest expected magnitude (the data's, never below a
+// physical floor) is mapped to [2^8, 2^9): 128x headroom before overflow,
+// full precision for values down to ~1e-7 of it
+double pick_scale(int storage, double maxabs, double floor_mag) {
     if (storage != LBF_STORE_F16 && storage != LBF_STORE_BF16) return 1.0;
-    double m = maxabs > 0 ? maxabs : fallback;
-    int e = (int)std::floor(std::log2(2048.0 / m));
+    double m = std::max(maxabs, floor_mag);
+    int e = (int)std::floor(std::log2(256.0 / m));
     return std::ldexp(1.0, e);
 }
+
+bool is_half(int storage) { return storage == LBF_STORE_F16 || storage == LBF_STORE_BF16; }
 
 }  // namespace
 
@@ -263,6 +270,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
         ok = ok && cudaMalloc(&h->mom[b], 10 * h->N * h->esz) == cudaSuccess;
         ok = ok && cudaMalloc(&h->uold[b], 3 * h->N * h->esz) == cudaSuccess;
         if (h->tc) ok = ok && cudaMalloc(&h->phi[b], h->N * h->psz) == cudaSuccess;
+        if (is_half(h->storage)) ok = ok && cudaMalloc(&h->pres[b], h->N * sizeof(float)) == cudaSuccess;
     }
     if (ok && h->obs) ok = cudaMalloc(&h->isf, h->N) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
@@ -400,28 +408,60 @@ int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype)
     if (h->obs && !h->isf_set) return fail(LBF_E_STATE, "obstacles: call lbf_set_isfluid before lbf_set_fields");
     const size_t hb = dtype == LBF_F64 ? 8 : 4;
     const long long N = h->N;
-    // per-field scales for 16-bit storage, from the data
-    if (h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16) {
-        const double fallback[10] = {1e-2, 1e-2, 1e-2, 1e-2, 1e-4, 1e-4, 1e-4, 1e-4, 1e-4, 1e-4};
-        for (int f = 0; f < 10; ++f) {
-            double m = 0;
-            for (long long i = 0; i < N; ++i) {
-                double v = dtype == LBF_F64 ? static_cast<const double*>(mom10)[f * N + i]
-                                            : static_cast<const float*>(mom10)[f * N + i];
-                if (std::isfinite(v)) m = std::max(m, std::fabs(v));
+    // 16-bit storage keeps Pi - u u (the deviation from equilibrium) with one
+    // power-of-two scale per group of fields: P, velocity, Pi - u u
+    std::vector<double> pin;  // Pi - u u, 6 x N, 16-bit modes only
+    const bool half = h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16;
+    if (half) {
+        auto at = [&](int f, long long i) -> double {
+            return dtype == LBF_F64 ? static_cast<const double*>(mom10)[f * N + i]
+                                    : (double)static_cast<const float*>(mom10)[f * N + i];
+        };
+        pin.resize(6 * (size_t)N);
+        const int ua[6] = {1, 2, 3, 1, 1, 2}, ub[6] = {1, 2, 3, 2, 3, 3};
+        double mP = 0, mU = 0, mPi = 0;
+        for (long long i = 0; i < N; ++i) {
+            double P = at(0, i);
+            if (std::isfinite(P)) mP = std::max(mP, std::fabs(P));
+            for (int f = 1; f <= 3; ++f) {
+                double v = at(f, i);
+                if (std::isfinite(v)) mU = std::max(mU, std::fabs(v));
             }
-            h->scale[f] = pick_scale(h->storage, m, fallback[f]);
+            for (int c = 0; c < 6; ++c) {
+                double v = at(4 + c, i) - at(ua[c], i) * at(ub[c], i);
+                pin[c * (size_t)N + i] = v;
+                if (std::isfinite(v)) mPi = std::max(mPi, std::fabs(v));
+            }
         }
-        for (int f = 0; f < 3; ++f) h->scale[lbf::NSCALE_H - 4 + f] = h->scale[1 + f];
+        (void)mP;  // P is stored in FP32 in the 16-bit modes
+        h->scale[0] = 1.0;
+        for (int f = 1; f <= 3; ++f) h->scale[f] = h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-2);
+        for (int f = 4; f < 10; ++f) h->scale[f] = pick_scale(h->storage, mPi, 1e-4);
     }
     int rc = ensure_staging(h, N * hb);
     if (rc) return rc;
     for (int f = 0; f < 10; ++f) {
         const char* src = static_cast<const char*>(mom10) + f * N * hb;
-        CUDA_TRY(cudaMemcpyAsync(h->staging, src, N * hb, cudaMemcpyHostToDevice, h->stream));
+        int sdt = dtype;
+        if (half && f >= 4) {
+            src = reinterpret_cast<const char*>(pin.data() + (size_t)(f - 4) * N);
+            sdt = LBF_F64;
+        }
+        const size_t sb = sdt == LBF_F64 ? 8 : 4;
+        if (sb > hb) {
+            rc = ensure_staging(h, N * sb);
+            if (rc) return rc;
+        }
+        CUDA_TRY(cudaMemcpyAsync(h->staging, src, N * sb, cudaMemcpyHostToDevice, h->stream));
+        // the host buffer of this field must not be reused before the copy ends
+        if (half && f >= 4) CUDA_TRY(cudaStreamSynchronize(h->stream));
         for (int b = 0; b < 2; ++b) {
             char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
-            CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, dst, N, h->scale[f], h->stream));
+            if (f == 0 && half) {
+                CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, sdt, h->pres[b], N, 1.0, h->stream));
+                continue;
+            }
+            CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, sdt, dst, N, h->scale[f], h->stream));
             if (f >= 1 && f <= 3) {  // u_old of the first step = initial velocity (B := A)
                 char* udst = static_cast<char*>(h->uold[b]) + (f - 1) * N * h->esz;
                 CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, udst, N,
@@ -465,6 +505,8 @@ int lbf_step(lbf_handle* h, int nsteps) {
     for (int i = 0; i < lbf::NSCALE_H; ++i) a.scale[i] = h->scale[i];
     a.isf = h->obs ? h->isf : nullptr;
     a.err = h->d_err;
+    a.pres_in = nullptr;
+    a.pres_out = nullptr;
     for (int s = 0; s < nsteps; ++s) {
         const int in = h->cur, out = 1 - h->cur;
         int rc = launch_wet(h, in, out, false);
@@ -475,6 +517,8 @@ int lbf_step(lbf_handle* h, int nsteps) {
         a.uout = h->uold[out];
         a.pin = h->phi[in];
         a.pout = h->phi[out];
+        a.pres_in = h->pres[in];
+        a.pres_out = h->pres[out];
         a.write_u = (h->dr || s == nsteps - 1) ? 1 : 0;
         cudaError_t e = h->launcher(a, h->stream);
         if (e != cudaSuccess) return fail(LBF_E_CUDA, "step kernel launch: %s", cudaGetErrorString(e));
@@ -516,12 +560,30 @@ int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype)
         CUDA_TRY(cudaStreamSynchronize(h->stream));
         return LBF_OK;
     };
-    if (mom10)
+    if (mom10) {
         for (int f = 0; f < 10; ++f) {
-            rc = out_field(static_cast<const char*>(h->mom[h->cur]) + f * N * h->esz, false, 1.0 / h->scale[f],
-                           static_cast<char*>(mom10) + f * N * hb);
+            if (f == 0 && is_half(h->storage))
+                rc = out_field(h->pres[h->cur], true, 1.0, mom10);
+            else
+                rc = out_field(static_cast<const char*>(h->mom[h->cur]) + f * N * h->esz, false, 1.0 / h->scale[f],
+                               static_cast<char*>(mom10) + f * N * hb);
             if (rc) return rc;
         }
+        if (h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16) {
+            // stored Pi - u u: add the equilibrium part back
+            const int ua[6] = {1, 2, 3, 1, 1, 2}, ub[6] = {1, 2, 3, 2, 3, 3};
+            for (int c = 0; c < 6; ++c)
+                for (long long i = 0; i < N; ++i) {
+                    if (dtype == LBF_F64) {
+                        double* m = static_cast<double*>(mom10);
+                        m[(4 + c) * N + i] += m[ua[c] * N + i] * m[ub[c] * N + i];
+                    } else {
+                        float* m = static_cast<float*>(mom10);
+                        m[(4 + c) * N + i] += m[ua[c] * N + i] * m[ub[c] * N + i];
+                    }
+                }
+        }
+    }
     if (phi && h->tc) {
         rc = out_field(h->phi[h->cur], true, 1.0, phi);
         if (rc) return rc;
@@ -559,7 +621,7 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press) {
     a.mode = !h->tc ? 0 : ((h->p.printphi || !h->dr) ? 1 : 2);
     a.rho_r = h->p.rho_r;
     a.rho_b = h->p.rho_b;
-    a.P = h->mom[src];
+    a.P = is_half(h->storage) ? static_cast<const void*>(h->pres[src]) : h->mom[src];
     a.sP = 1.0 / h->scale[0];
     if (h->step == 0) {
         a.vel = static_cast<const char*>(h->mom[h->cur]) + 1 * N * h->esz;
@@ -587,7 +649,7 @@ int lbf_reduce(lbf_handle* h, double out[5]) {
     if (!h->fields_set) return fail(LBF_E_STATE, "lbf_reduce before lbf_set_fields");
     double inv[4];
     for (int f = 0; f < 4; ++f) inv[f] = 1.0 / h->scale[f];
-    CUDA_TRY(lbf::launch_reduce(h->storage, h->N, h->mom[h->cur], h->tc ? h->phi[h->cur] : nullptr,
+    CUDA_TRY(lbf::launch_reduce(h->storage, h->N, h->mom[h->cur], h->pres[h->cur], h->tc ? h->phi[h->cur] : nullptr,
                                 h->obs ? h->isf : nullptr, inv, h->d_red, h->stream));
     CUDA_TRY(cudaMemcpyAsync(out, h->d_red, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));

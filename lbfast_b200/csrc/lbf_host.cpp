@@ -2,9 +2,15 @@
 // the C ABI (include/lbfast_gpu.h): isfluid marking, initial conditions and
 // the raw/XDMF writer.  These run once per run (or per output frame) on the
 // CPU, as in the reference.
+#include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -112,9 +118,13 @@ int lbf_ic_taylor_green(int lx, int ly, int lz, double u0, double* m) {
     return LBF_OK;
 }
 
-// init_conditions_module.f90:394-426 with pbc_images (:591-600)
-int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
-                   double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* m, double* phi) {
+}  // extern "C"
+
+namespace {
+// droplet of init_conditions_module.f90:355-426; xscale = 0.5 is the LAMBTEST
+// ellipsoid (dist3dout(1)*HALF, :362)
+int droplet(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
+            double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* m, double* phi, double xscale) {
     if (!center || !m || !phi || radius <= 0 || width <= 0) return LBF_E_ARG;
     const long long N = (long long)lx * ly * lz;
     for (long long c = 0; c < 10 * N; ++c) m[c] = 0.0;
@@ -127,6 +137,7 @@ int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius
                 double d[3] = {(i + 1) - center[0], (j + 1) - center[1], (k + 1) - center[2]};
                 const int L[3] = {lx, ly, lz};
                 for (int a = 0; a < 3; ++a) d[a] = d[a] - L[a] * nint_f(d[a] / L[a]);
+                d[0] *= xscale;
                 double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
                 double ph = 0.5 * (1.0 - std::tanh((r - radius) / (0.5 * width)));
                 double rp = densratio ? rho_r * ph + (1.0 - ph) * rho_b : 1.0;
@@ -134,6 +145,21 @@ int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius
                 phi[c] = ph;
             }
     return LBF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+// init_conditions_module.f90:394-426 with pbc_images (:591-600)
+int lbf_ic_droplet(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
+                   double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* m, double* phi) {
+    return droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio, isfluid, m, phi, 1.0);
+}
+
+// init_conditions_module.f90:355-393
+int lbf_ic_lamb(int lx, int ly, int lz, const double center[3], double radius, double width, double sigma,
+                double rho_r, double rho_b, int densratio, const int8_t* isfluid, double* m, double* phi) {
+    return droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio, isfluid, m, phi, 0.5);
 }
 
 // print_raw_sync, print_module.f90:2007-2180 (float32 stream files + XDMF)
@@ -194,3 +220,218 @@ int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Fortran namelist reader for the reference's `simulation` / `fluid` groups
+// (LBFAST.f90:32-60): `&group`, `key = value[, value...]`, `!` comments,
+// `.true.` / `.false.`, reals with e or d exponents, terminated by `&end` or `/`.
+// ---------------------------------------------------------------------------
+namespace {
+
+std::string lower(std::string s) {
+    for (char& c : s) c = (char)std::tolower((unsigned char)c);
+    return s;
+}
+std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+struct NmlError {
+    std::string msg;
+};
+
+// split "a = 1, b = 2.0" style text into key -> list of raw values
+std::vector<std::pair<std::string, std::vector<std::string>>> parse_group(const std::string& body) {
+    std::vector<std::pair<std::string, std::vector<std::string>>> out;
+    // tokens separated by commas / whitespace; a key is a token followed by '='
+    std::string s = body;
+    for (char& c : s)
+        if (c == '\n' || c == '\r' || c == '\t') c = ' ';
+    size_t i = 0;
+    std::string key;
+    std::vector<std::string> vals;
+    auto flush = [&]() {
+        if (!key.empty()) out.push_back({key, vals});
+        key.clear();
+        vals.clear();
+    };
+    while (i < s.size()) {
+        while (i < s.size() && (s[i] == ' ' || s[i] == ',')) ++i;
+        if (i >= s.size()) break;
+        size_t j = i;
+        while (j < s.size() && s[j] != ' ' && s[j] != ',' && s[j] != '=') ++j;
+        std::string tok = s.substr(i, j - i);
+        size_t k = j;
+        while (k < s.size() && s[k] == ' ') ++k;
+        if (k < s.size() && s[k] == '=') {
+            flush();
+            key = lower(tok);
+            size_t p = key.find('(');
+            if (p != std::string::npos) key = key.substr(0, p);  // element assignment key(1)=
+            i = k + 1;
+        } else {
+            if (key.empty()) throw NmlError{"value `" + tok + "` without a key"};
+            vals.push_back(tok);
+            i = j;
+        }
+    }
+    flush();
+    return out;
+}
+
+double to_real(const std::string& v, const std::string& key) {
+    std::string t = lower(v);
+    std::replace(t.begin(), t.end(), 'd', 'e');
+    char* end = nullptr;
+    double x = std::strtod(t.c_str(), &end);
+    if (end == t.c_str() || *end != '\0') throw NmlError{"bad real `" + v + "` for " + key};
+    return x;
+}
+int to_int(const std::string& v, const std::string& key) {
+    char* end = nullptr;
+    long x = std::strtol(v.c_str(), &end, 10);
+    if (end == v.c_str() || *end != '\0') throw NmlError{"bad integer `" + v + "` for " + key};
+    return (int)x;
+}
+int to_bool(const std::string& v, const std::string& key) {
+    std::string t = lower(v);
+    if (t == ".true." || t == "t" || t == ".t.") return 1;
+    if (t == ".false." || t == "f" || t == ".f.") return 0;
+    throw NmlError{"bad logical `" + v + "` for " + key};
+}
+
+// body of group `name` (text between `&name` and `&end` or `/`), comments removed
+std::string group_body(const std::string& text, const std::string& name) {
+    std::istringstream in(text);
+    std::string line, body;
+    bool inside = false;
+    while (std::getline(in, line)) {
+        size_t c = line.find('!');
+        if (c != std::string::npos) line = line.substr(0, c);
+        std::string t = lower(trim(line));
+        if (!inside) {
+            if (t.rfind("&" + name, 0) == 0) {
+                inside = true;
+                body += line.substr(line.find('&') + 1 + name.size()) + "\n";
+            }
+            continue;
+        }
+        if (t.rfind("&end", 0) == 0 || t == "/") return body;
+        size_t slash = line.find('/');
+        if (slash != std::string::npos) return body + line.substr(0, slash);
+        body += line + "\n";
+    }
+    if (!inside) throw NmlError{"namelist group &" + name + " not found"};
+    throw NmlError{"namelist group &" + name + " is not terminated"};
+}
+
+}  // namespace
+
+extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run) {
+    if (!path || !p || !run) return LBF_E_ARG;
+    std::ifstream f(path);
+    if (!f) {
+        std::fprintf(stderr, "lbf_read_namelists: cannot open %s\n", path);
+        return LBF_E_IO;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    // DOBENCHMARK defaults, LBFAST.f90:159-191
+    run->nsteps = 100; run->stamp = 100; run->stamp2D = 10; run->stamp_term = 2147483647; run->stepskip = 1;
+    run->lreadisfluid = 0; run->lreadinit = 0; run->lprint = 1; run->lvtk = 0; run->lraw = 1; run->lrestart = 0;
+    run->lwriterestart = 0; run->openbc = 0; run->nplanes = 0; run->every_time_check = 1000;
+    run->iprobe = run->jprobe = run->kprobe = 0;
+    run->time_limit = -1.0;
+    run->uwall = 0.0;
+    run->width = 0.0;
+    run->center[0] = run->center[1] = run->center[2] = 0.0;
+    p->lx = p->ly = p->lz = 512;
+    p->pbc_x = p->pbc_y = p->pbc_z = 1;
+    p->fx = p->fy = p->fz = 0.0;
+    p->rho_r = p->rho_b = 1.0;  // vars_module.f90:775
+    p->visc1 = p->visc2 = 0.0;
+    p->sigma = 0.0;
+    p->width = 0.0;
+    p->tau_diff = 0.0;
+    p->wettab_r = 90.0;
+    try {
+        for (auto& kv : parse_group(group_body(text, "simulation"))) {
+            const std::string& k = kv.first;
+            const auto& v = kv.second;
+            if (v.empty()) throw NmlError{"no value for " + k};
+            const std::string& a = v[0];
+            if (k == "nsteps") run->nsteps = to_int(a, k);
+            else if (k == "stamp") run->stamp = to_int(a, k);
+            else if (k == "stamp2d") run->stamp2D = to_int(a, k);
+            else if (k == "stamp_term") run->stamp_term = to_int(a, k);
+            else if (k == "stepskip") run->stepskip = to_int(a, k);
+            else if (k == "lreadisfluid") run->lreadisfluid = to_bool(a, k);
+            else if (k == "lreadinit") run->lreadinit = to_bool(a, k);
+            else if (k == "lx") p->lx = to_int(a, k);
+            else if (k == "ly") p->ly = to_int(a, k);
+            else if (k == "lz") p->lz = to_int(a, k);
+            else if (k == "lprint") run->lprint = to_bool(a, k);
+            else if (k == "lvtk") run->lvtk = to_bool(a, k);
+            else if (k == "lraw") run->lraw = to_bool(a, k);
+            else if (k == "lrestart") run->lrestart = to_bool(a, k);
+            else if (k == "lwriterestart") run->lwriterestart = to_bool(a, k);
+            else if (k == "pbc_x") p->pbc_x = to_int(a, k);
+            else if (k == "pbc_y") p->pbc_y = to_int(a, k);
+            else if (k == "pbc_z") p->pbc_z = to_int(a, k);
+            else if (k == "openbc") run->openbc = to_int(a, k);
+            else if (k == "iprobe") run->iprobe = to_int(a, k);
+            else if (k == "jprobe") run->jprobe = to_int(a, k);
+            else if (k == "kprobe") run->kprobe = to_int(a, k);
+            else if (k == "nplanes") run->nplanes = to_int(a, k);
+            else if (k == "time_limit") run->time_limit = to_real(a, k);
+            else if (k == "every_time_check") run->every_time_check = to_int(a, k);
+            else if (k == "lasync" || k == "lweakscaling") to_bool(a, k);
+            else if (k.rfind("openbc_type_", 0) == 0) { for (auto& x : v) to_int(x, k); }
+            else if (k.rfind("openbc_", 0) == 0) { for (auto& x : v) to_real(x, k); }
+            else throw NmlError{"unknown key `" + k + "` in &simulation"};
+        }
+        bool have_radius = false;
+        for (auto& kv : parse_group(group_body(text, "fluid"))) {
+            const std::string& k = kv.first;
+            const auto& v = kv.second;
+            if (v.empty()) throw NmlError{"no value for " + k};
+            const std::string& a = v[0];
+            if (k == "fx") p->fx = to_real(a, k);
+            else if (k == "fy") p->fy = to_real(a, k);
+            else if (k == "fz") p->fz = to_real(a, k);
+            else if (k == "visc1") p->visc1 = to_real(a, k);
+            else if (k == "visc2") p->visc2 = to_real(a, k);
+            else if (k == "radius") { run->radius = to_real(a, k); have_radius = true; }
+            else if (k == "width") { run->width = to_real(a, k); p->width = run->width; }
+            else if (k == "center") {
+                if (v.size() != 3) throw NmlError{"center needs 3 values"};
+                for (int d = 0; d < 3; ++d) run->center[d] = to_real(v[d], k);
+            } else if (k == "tau_diff") p->tau_diff = to_real(a, k);
+            else if (k == "sigma") p->sigma = to_real(a, k);
+            else if (k == "wettab_r") p->wettab_r = to_real(a, k);
+            else if (k == "rho_r") p->rho_r = to_real(a, k);
+            else if (k == "rho_b") p->rho_b = to_real(a, k);
+            else if (k == "uwall") run->uwall = to_real(a, k);
+            else if (k == "wettab_b" || k == "mu_max" || k == "ks" || k == "k_elastic" || k == "lambda_rel" ||
+                     k == "rhoin" || k == "rhoout" || k == "a_rep" || k == "cosoppt" || k == "q_th") {
+                for (auto& x : v) to_real(x, k);
+            } else if (k == "npoint" || k == "ndir") { for (auto& x : v) to_int(x, k); }
+            else throw NmlError{"unknown key `" + k + "` in &fluid"};
+        }
+        if (!have_radius) run->radius = p->lx / 4;  // DOBENCHMARK: radius = lx/4 (integer division)
+    } catch (const NmlError& e) {
+        std::fprintf(stderr, "lbf_read_namelists: %s: %s\n", path, e.msg.c_str());
+        return LBF_E_ARG;
+    }
+    if (run->openbc != 0) {
+        std::fprintf(stderr, "lbf_read_namelists: openbc = %d: open boundaries are not supported\n", run->openbc);
+        return LBF_E_UNSUPPORTED;
+    }
+    if (run->lrestart) {
+        std::fprintf(stderr, "lbf_read_namelists: lrestart: restart files are not supported\n");
+        return LBF_E_UNSUPPORTED;
+    }
+    return LBF_OK;
+}

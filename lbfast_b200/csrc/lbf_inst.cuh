@@ -39,6 +39,8 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     p.uout = static_cast<S*>(a.uout);
     p.pin = static_cast<const SP*>(a.pin);
     p.pout = static_cast<SP*>(a.pout);
+    p.pres_in = a.pres_in;
+    p.pres_out = a.pres_out;
     p.isf = a.isf;
     p.err = a.err;
     dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zseg - 1) / a.zseg);

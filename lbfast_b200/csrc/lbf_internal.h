@@ -20,6 +20,8 @@ struct StepArgs {
     void* uout;
     const void* pin;
     void* pout;
+    const float* pres_in;   // P with 16-bit storage
+    float* pres_out;
     const int8_t* isf;
     int* err;
 };
@@ -64,7 +66,7 @@ struct PrintArgs {
     long long N;
     int mode;            // 0: P, 1: phi, 2: rho_phi
     double rho_r, rho_b;
-    const void* P;       // moment field 0
+    const void* P;       // moment field 0 (float array with 16-bit storage)
     const void* vel;     // 3 consecutive velocity fields
     const void* phi;
     double sP, su[3];    // inverse scales
@@ -75,8 +77,8 @@ struct PrintArgs {
 cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
 
 // FP64 reductions over fluid nodes: out[5] = {sum phi, sum P, sum u, sum v, sum w}
-cudaError_t launch_reduce(int storage, long long N, const void* mom, const void* phi, const int8_t* isf,
-                          const double* inv_scale, double* d_out, cudaStream_t st);
+cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
+                          const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st);
 
 size_t storage_bytes(int storage);
 

@@ -95,8 +95,10 @@ template <> struct Codec<__nv_bfloat16> {
     }
 };
 
-// phi keeps 32-bit storage when the moments are stored in 16 bits: it lives in
-// [0,1] and a 16-bit mantissa cannot resolve its interface profile.
+// phi and P keep 32-bit storage when the other moments are stored in 16 bits:
+// phi lives in [0,1] and a 16-bit mantissa cannot resolve its interface
+// profile; P is conserved, so its rounding errors add up step after step
+// instead of relaxing away as the velocity's and Pi's do.
 template <typename S> struct PhiStore { using type = S; };
 template <> struct PhiStore<__half> { using type = float; };
 template <> struct PhiStore<__nv_bfloat16> { using type = float; };
@@ -116,8 +118,10 @@ template <typename S, typename R> struct StepParams {
     int zseg;         // planes per z segment
     R omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     R scale[NSCALE], inv_scale[NSCALE];
-    const S* min;     // 10 x N moments, input
+    const S* min;     // 10 x N moments, input (field 0 unused with 16-bit storage)
     S* mout;          // 10 x N moments, output
+    const float* pres_in;  // N pressure moment P, input (16-bit storage only)
+    float* pres_out;       // N pressure moment P, output (16-bit storage only)
     const S* uin;     // 3 x N velocity of the previous step (DENSRATIO)
     S* uout;          // 3 x N velocity after the force half-step
     const typename PhiStore<S>::type* pin;  // N phase field, input

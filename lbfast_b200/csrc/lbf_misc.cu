@@ -1,6 +1,8 @@
 // lbf_misc.cu -- the small kernels around the fused step: wetting ghost phi,
 // field conversions at the host boundary, copy_print extraction and FP64
 // reductions.
+#include <type_traits>
+
 #include "lbf_internal.h"
 #include "lbf_stream.cuh"
 
@@ -182,11 +184,13 @@ cudaError_t launch_convert_out(int storage, bool is_phi, const void* src, void* 
 template <typename S, typename R>
 __global__ void print_kernel(const PrintArgs a) {
     using SP = typename PhiStore<S>::type;
-    const S* P = static_cast<const S*>(a.P);
+    // with 16-bit storage P is a float array (PhiStore<S> is float there too)
+    using SPres = typename std::conditional<Codec<S>::scaled, float, S>::type;
+    const SPres* P = static_cast<const SPres*>(a.P);
     const S* V = static_cast<const S*>(a.vel);
     const SP* ph = static_cast<const SP*>(a.phi);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
-        R press = Codec<S>::ld(P, i, (R)a.sP);
+        R press = Codec<SPres>::ld(P, i, (R)a.sP);
         if (a.rho) {
             R r;
             if (a.mode == 0) r = press;
@@ -219,8 +223,8 @@ cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st) {
 // with a block-level tree instead of one atomic per node)
 // ---------------------------------------------------------------------------
 template <typename S>
-__global__ void reduce_kernel(long long N, const S* mom, const typename PhiStore<S>::type* phi, const int8_t* isf,
-                              double s0, double s1, double s2, double s3, double* out) {
+__global__ void reduce_kernel(long long N, const S* mom, const float* pres, const typename PhiStore<S>::type* phi,
+                              const int8_t* isf, double s0, double s1, double s2, double s3, double* out) {
     using SP = typename PhiStore<S>::type;
     double acc[5] = {0, 0, 0, 0, 0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
@@ -229,7 +233,7 @@ __global__ void reduce_kernel(long long N, const S* mom, const typename PhiStore
             if (f != 1 && f != -1) continue;
         }
         if (phi) acc[0] += (double)Codec<SP>::ld(phi, i, 1.0);
-        acc[1] += (double)Codec<S>::ld(mom, i, s0);
+        acc[1] += pres ? (double)pres[i] : (double)Codec<S>::ld(mom, i, s0);
         acc[2] += (double)Codec<S>::ld(mom, N + i, s1);
         acc[3] += (double)Codec<S>::ld(mom, 2 * N + i, s2);
         acc[4] += (double)Codec<S>::ld(mom, 3 * N + i, s3);
@@ -249,14 +253,14 @@ __global__ void reduce_kernel(long long N, const S* mom, const typename PhiStore
         for (int k = 0; k < 5; ++k) atomicAdd(out + k, red[k][0]);
 }
 
-cudaError_t launch_reduce(int storage, long long N, const void* mom, const void* phi, const int8_t* isf,
-                          const double* inv_scale, double* d_out, cudaStream_t st) {
+cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
+                          const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(d_out, 0, 5 * sizeof(double), st);
     if (e != cudaSuccess) return e;
     return by_storage(storage, [&](auto tag) {
         using S = decltype(tag);
         using SP = typename PhiStore<S>::type;
-        reduce_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(N, static_cast<const S*>(mom),
+        reduce_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(N, static_cast<const S*>(mom), pres,
                                                               static_cast<const SP*>(phi), isf, inv_scale[0],
                                                               inv_scale[1], inv_scale[2], inv_scale[3], d_out);
         return cudaGetLastError();

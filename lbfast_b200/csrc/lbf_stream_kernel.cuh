@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(co
                     pxx = (R)stg[4 * R1N + node]; pyy = (R)stg[5 * R1N + node]; pzz = (R)stg[6 * R1N + node];
                     pxy = (R)stg[7 * R1N + node]; pxz = (R)stg[8 * R1N + node]; pyz = (R)stg[9 * R1N + node];
                 } else {
-                    P = CD::ld(p.min, 0 * N + gi, p.inv_scale[0]);
+                    P = (R)__ldg(p.pres_in + gi);
                     u = CD::ld(p.min, 1 * N + gi, p.inv_scale[1]);
                     v = CD::ld(p.min, 2 * N + gi, p.inv_scale[2]);
                     w = CD::ld(p.min, 3 * N + gi, p.inv_scale[3]);
@@ -308,6 +308,11 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(co
                     pxy = CD::ld(p.min, 7 * N + gi, p.inv_scale[7]);
                     pxz = CD::ld(p.min, 8 * N + gi, p.inv_scale[8]);
                     pyz = CD::ld(p.min, 9 * N + gi, p.inv_scale[9]);
+                    if constexpr (CD::scaled) {
+                        // 16-bit storage keeps Pi - u u, the deviation from equilibrium
+                        pxx += u * u; pyy += v * v; pzz += w * w;
+                        pxy += u * v; pxz += u * w; pyz += v * w;
+                    }
                 }
                 R phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
                 if constexpr (TC) {
@@ -592,7 +597,12 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(co
         if (q - 1 >= z0 && out_ok) {
             const long long go = (long long)(q - 1) * plane + out_off;
             const R third = am[0] * cssq;
-            CD::st(p.mout, 0 * N + go, am[0], p.scale[0]);
+            if constexpr (CD::scaled) {
+                am[4] -= am[1] * am[1]; am[5] -= am[2] * am[2]; am[6] -= am[3] * am[3];
+                am[7] -= am[1] * am[2]; am[8] -= am[1] * am[3]; am[9] -= am[2] * am[3];
+            }
+            if constexpr (CD::scaled) p.pres_out[go] = (float)am[0];
+            else CD::st(p.mout, 0 * N + go, am[0], p.scale[0]);
             CD::st(p.mout, 1 * N + go, am[1], p.scale[1]);
             CD::st(p.mout, 2 * N + go, am[2], p.scale[2]);
             CD::st(p.mout, 3 * N + go, am[3], p.scale[3]);

@@ -1,0 +1,165 @@
+"""Physics-level checks on the GPU: 16-bit storage against the FP64 oracle,
+the reference's analytic benchmarks (statistics.f90: Taylor-Green viscous
+decay, Laplace law), the Taylor-Green configuration of the reference's CPU
+case against the oracle, and the C++ driver end to end."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from cases import make_case, rel_l2, run_oracle
+import lbfast_b200 as L
+from lbfast_b200 import statistics as ST
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(name, storage, n):
+    p, isf, m, phi = make_case(name, storage)
+    s = L.Solver(p)
+    if p.obstacles:
+        s.set_isfluid(isf)
+    s.set_fields(m, phi)
+    s.step(n)
+    out = s.get_fields()
+    s.close()
+    return p, isf, out
+
+
+def _fp16_errors(name, n=100):
+    o = run_oracle(name, n, "f64")
+    mo, po, _ = o.get_fields()
+    p, isf, (mg, pg, _) = _run(name, "f16", n)
+    fl = np.abs(isf) == 1
+    err = {"P": rel_l2(mg[0:1], mo[0:1], fl), "u": rel_l2(mg[1:4], mo[1:4], fl),
+           "Pi": rel_l2(mg[4:10], mo[4:10], fl)}
+    if p.twocomponent:
+        err["phi"] = rel_l2(pg, po, fl)
+    return err
+
+
+@pytest.mark.parametrize("name", ["q27ho_2c_dr", "obs_q27ho_2c_dr"])
+def test_fp16_storage_two_component_within_1e3(name):
+    """16-bit storage (u, u_old and Pi - u u in FP16, one power-of-two scale per
+    field group; P and phi in FP32; FP32 arithmetic) after 100 steps against the
+    FP64 oracle: the observables P, u and phi within 1e-3 rel-L2, Pi within 3e-3."""
+    err = _fp16_errors(name)
+    assert err["P"] <= 1e-3 and err["u"] <= 1e-3 and err["phi"] <= 1e-3 and err["Pi"] <= 3e-3, err
+
+
+@pytest.mark.parametrize("name", ["q27ho_1c_force", "tg_q19"])
+def test_fp16_storage_one_component(name):
+    """One component: u within 1e-3; P, second order in u (the pressure answers
+    the velocity's divergence, so FP16 rounding noise in u shows up amplified in
+    P), within 3e-3; Pi within 5e-3."""
+    err = _fp16_errors(name)
+    assert err["u"] <= 1e-3 and err["P"] <= 3e-3 and err["Pi"] <= 5e-3, err
+
+
+@pytest.mark.parametrize("name", ["q27ho_2c_dr", "tg_q19"])
+def test_bf16_storage_is_finite_and_close(name):
+    """BF16 keeps 8 mantissa bits: finite and within 5e-2 of the FP64 oracle."""
+    n = 100
+    o = run_oracle(name, n, "f64")
+    mo, po, _ = o.get_fields()
+    p, isf, (mg, pg, _) = _run(name, "bf16", n)
+    assert np.all(np.isfinite(mg))
+    assert rel_l2(mg, mo) < 5e-2
+
+
+def test_taylor_green_viscous_decay_linear_regime():
+    """statistics.f90:918-956 on the GPU: 64^3 D3Q19, nu = 0.01, u0 = 5e-4
+    (Re << 1, where E/E0 = exp(-6 nu k^2 t) holds): fitted nu within 1%."""
+    n, nu = 64, 0.01
+    s = L.Solver(L.Params(lx=n, ly=n, lz=n, lattice=19, visc1=nu))
+    s.set_fields(L.ic_taylor_green(n, n, n, 5e-4))
+    t, e = [], []
+    for _ in range(11):
+        _, vel, _ = s.get_print()
+        t.append(s.nstep)
+        e.append(ST.kinetic_energy(vel))
+        s.step(100)
+    s.close()
+    t, e = np.array(t[1:]), np.array(e[1:])  # after the start-up transient of the regularised IC
+    assert abs(ST.fit_viscosity(t, e, n) / nu - 1) < 0.01
+
+
+def test_taylor_green_config_matches_oracle():
+    """The reference's CPU case (64^3 D3Q19, nu = 0.01, u0 = 0.05): FP32 GPU
+    within 1e-5 rel-L2 of the FP64 oracle after 200 steps."""
+    n = 64
+    p = L.Params(lx=n, ly=n, lz=n, lattice=19, visc1=0.01)
+    m = L.ic_taylor_green(n, n, n, 0.05)
+    s = L.Solver(p)
+    s.set_fields(m)
+    s.step(200)
+    mg, _, _ = s.get_fields()
+    s.close()
+    from oracle import oracle as O
+    o = O.Oracle(p.oracle_dict(), "f64")
+    o.set_isfluid(np.ones(p.shape, np.int8))
+    o.set_fields(m)
+    o.step(200)
+    mo, _, _ = o.get_fields()
+    assert rel_l2(mg, mo) < 1e-5
+
+
+def test_laplace_law():
+    """statistics.f90:88-275 on a 128^3 droplet, R = 20, density ratio 100:
+    the pressure jump settles (sigma_eff steady to 1% over the last 1000
+    steps) and sigma_eff = dp R / 2 is within 30% of sigma (a width-3
+    interface; the deviation is the scheme's)."""
+    n, R, sig = 128, 20.0, 0.03
+    p = L.Params(lx=n, ly=n, lz=n, lattice=27, highorder=1, twocomponent=1, densratio=1, visc1=0.1, visc2=0.1,
+                 rho_r=100.0, rho_b=1.0, sigma=sig, width=3.0, tau_diff=0.1, printphi=1)
+    c = (n / 2, n / 2, n / 2)
+    m, phi = L.ic_droplet(n, n, n, c, R, 3.0, sig, 100.0, 1.0, True)
+    s = L.Solver(p)
+    s.set_fields(m, phi)
+    vals = []
+    for _ in range(4):
+        s.step(1000)
+        rho, vel, press = s.get_print()
+        vals.append(ST.laplace_observables(rho, press, c, (1, n // 2, n // 2), 100.0, 1.0))
+        assert np.all(np.isfinite(vel))
+    s.close()
+    se = [v[0] for v in vals]
+    assert abs(se[-1] / se[-2] - 1) < 0.01, se
+    assert abs(se[-1] / sig - 1) < 0.3, se
+    assert abs(vals[-1][2] - R) < 1.0
+
+
+def test_driver_matches_library(tmp_path):
+    """lbfast_b200/_lib/lbfast on a channel with walls, a droplet and
+    obstacles-enabled wetting: runs, writes the reference's output files, and
+    its last frame equals the same run driven through the Python binding."""
+    exe = os.path.join(ROOT, "lbfast_b200", "_lib", "lbfast")
+    shutil.copy(os.path.join(ROOT, "tests", "golden", "channel.inp"), tmp_path / "channel.inp")
+    flags = ["-DLATTICE=27", "-DHIGHORDER", "-DTWOCOMPONENT", "-DDENSRATIO", "-DINTERNAL_OBSTACLES", "-DPRINTPHI"]
+    r = subprocess.run([exe, *flags, "channel.inp"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "glups:" in r.stdout and "program correctly closed" in r.stdout
+    out = tmp_path / "output"
+    for f in ("out_rho_000000.raw", "out_vel_000002.raw", "out_rho_000002.xdmf"):
+        assert (out / f).exists(), f
+    lx, ly, lz = 36, 20, 24
+    rho_drv = np.fromfile(out / "out_rho_000002.raw", dtype=np.float32).reshape(lz, ly, lx)
+    vel_drv = np.fromfile(out / "out_vel_000002.raw", dtype=np.float32).reshape(lz, ly, lx, 3)
+    # the same run through the binding
+    isf = L.mark_isfluid(np.ones((lz, ly, lx), np.int8), (1, 0, 1), 27, True)
+    m, phi = L.ic_droplet(lx, ly, lz, (18.0, 10.0, 12.0), 6.0, 4.0, 0.01, 0.5, 1.5, True, isf)
+    phi = L.seed_solid_phi(phi, isf, 27)
+    p = L.Params(lx=lx, ly=ly, lz=lz, pbc_y=0, lattice=27, highorder=1, twocomponent=1, densratio=1, obstacles=1,
+                 visc1=0.05, visc2=0.2, rho_r=0.5, rho_b=1.5, sigma=0.01, width=4.0, tau_diff=0.1, fx=1e-5,
+                 wettab_r=90.0, printphi=1)
+    s = L.Solver(p)
+    s.set_isfluid(isf)
+    s.set_fields(m, phi)
+    s.step(40)
+    rho, vel, _ = s.get_print()
+    s.close()
+    assert np.array_equal(rho_drv, rho, equal_nan=True)
+    assert np.array_equal(vel_drv, np.moveaxis(vel, 0, -1))

@@ -1,0 +1,148 @@
+"""Host side of the library (no GPU): the C ABI loads and exports every
+declared symbol, the set-up helpers agree with the oracle's restatements of
+the reference, the namelist reader accepts the reference's input format, the
+raw/XDMF writer produces the reference's files, and invalid parameters are
+rejected before any device work."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from cases import _spheres_solid
+from lbfast_b200 import capi
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "lbfast_gpu.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lbf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    lib = capi.load()
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+class Run(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("nsteps stamp stamp2D stamp_term stepskip lreadisfluid lreadinit lprint "
+                                       "lvtk lraw lrestart lwriterestart openbc nplanes every_time_check iprobe "
+                                       "jprobe kprobe").split()] + \
+               [("time_limit", C.c_double), ("uwall", C.c_double), ("radius", C.c_double), ("width", C.c_double),
+                ("center", C.c_double * 3)]
+
+
+def read_nml(path):
+    lib = capi.load()
+    lib.lbf_read_namelists.argtypes = [C.c_char_p, C.POINTER(capi.LbfParams), C.POINTER(Run)]
+    p = capi.LbfParams()
+    r = Run()
+    rc = lib.lbf_read_namelists(str(path).encode(), C.byref(p), C.byref(r))
+    return rc, p, r
+
+
+@pytest.mark.parametrize("pbc", [(1, 1, 1), (1, 0, 1), (0, 1, 0)])
+@pytest.mark.parametrize("lattice", [19, 27])
+def test_mark_isfluid_matches_restatement(pbc, lattice):
+    rng = np.random.default_rng(11 + lattice)
+    solid = _spheres_solid(rng, (14, 18, 22), 3, 2.0, 3.5)
+    a = capi.mark_isfluid((~solid).astype(np.int8), pbc, lattice, True)
+    b = O.mark_isfluid(solid, pbc, lattice, True)
+    assert np.array_equal(a, b)
+    assert (a == -1).sum() > 0
+
+
+def test_initial_conditions_match_restatement():
+    m = capi.ic_taylor_green(32, 24, 16, 0.05)
+    assert np.allclose(m, O.ic_taylor_green(32, 24, 16, 0.05), rtol=0, atol=1e-15)
+    m, phi = capi.ic_droplet(40, 24, 28, (20.5, 12, 14.5), 7, 3, 0.03, 1.0, 0.1, True)
+    m2, phi2 = O.ic_droplet(40, 24, 28, (20.5, 12, 14.5), 7, 3, 0.03, 1.0, 0.1, True)
+    assert np.allclose(m, m2, rtol=1e-14, atol=1e-16) and np.allclose(phi, phi2, rtol=1e-14, atol=1e-16)
+    # the droplet straddles the periodic faces: nearest-image distance
+    m, phi = capi.ic_droplet(24, 24, 24, (1.0, 23.0, 12.0), 5, 3, 0.03, 1.0, 0.1, True)
+    assert phi[11, 22, 0] > 0.99 and phi[11, 0, 1] > 0.5
+
+
+def test_seed_solid_phi_matches_restatement_including_nan():
+    rng = np.random.default_rng(5)
+    isf = O.mark_isfluid(_spheres_solid(rng, (12, 16, 20), 3, 2.0, 3.5), (1, 1, 1), 27, True)
+    phi = rng.random(isf.shape)
+    a = capi.seed_solid_phi(phi, isf, 27)
+    b = O.seed_solid_phi(phi, isf, 27)
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    assert np.nanmax(np.abs(a - b)) < 1e-15
+
+
+def test_namelist_reader_defaults_and_values():
+    rc, p, r = read_nml(os.path.join(ROOT, "tests", "golden", "channel.inp"))
+    assert rc == 0
+    assert (p.lx, p.ly, p.lz, p.pbc_x, p.pbc_y, p.pbc_z) == (36, 20, 24, 1, 0, 1)
+    assert p.fx == 1e-5 and p.visc1 == 0.05 and p.visc2 == 0.2 and p.rho_r == 0.5 and p.rho_b == 1.5
+    assert p.sigma == 0.01 and p.width == 4.0 and p.tau_diff == 0.1 and p.wettab_r == 60.0
+    assert (r.nsteps, r.stamp, r.stamp_term, r.iprobe, r.jprobe, r.kprobe) == (40, 20, 10, 5, 10, 12)
+    assert list(r.center) == [18.0, 10.0, 12.0] and r.radius == 6.0
+    assert r.time_limit == -1.0 and r.every_time_check == 1000  # vars_module.f90:777-779
+
+
+def test_namelist_reader_rejects_bad_input(tmp_path):
+    base = open(os.path.join(ROOT, "tests", "golden", "channel.inp")).read()
+    cases = {"unknown": base.replace("lx=36", "lx=36\n   bogus_key=3"),
+             "badreal": base.replace("fx=1.0d-5", "fx=1.0x-5"),
+             "openbc": base.replace("openbc=0", "openbc=1"),
+             "nofluid": base.split("&fluid")[0]}
+    for name, text in cases.items():
+        f = tmp_path / f"{name}.inp"
+        f.write_text(text)
+        rc, _, _ = read_nml(f)
+        assert rc != 0, name
+
+
+def test_namelist_reader_reads_reference_inputs():
+    ref = "/root/reference"
+    files = sorted(f for f in os.listdir(ref) if f.endswith(".inp")) if os.path.isdir(ref) else []
+    if not files:
+        pytest.skip("reference inputs not mounted")
+    for f in files:
+        rc, p, r = read_nml(os.path.join(ref, f))
+        assert rc == 0, f
+        assert p.lx > 0 and r.nsteps > 0
+
+
+def test_raw_xdmf_writer(tmp_path):
+    lz, ly, lx = 3, 4, 5
+    rho = np.arange(lx * ly * lz, dtype=np.float32).reshape(lz, ly, lx)
+    vel = np.stack([rho, -rho, 2 * rho])
+    capi.write_raw_xdmf(str(tmp_path), 7, rho, vel, rho + 1)
+    names = sorted(os.listdir(tmp_path))
+    assert names == ["out_press_000007.raw", "out_press_000007.xdmf", "out_rho_000007.raw", "out_rho_000007.xdmf",
+                     "out_vel_000007.raw", "out_vel_000007.xdmf"]
+    r = np.fromfile(tmp_path / "out_rho_000007.raw", dtype=np.float32)
+    assert np.array_equal(r, rho.ravel())
+    v = np.fromfile(tmp_path / "out_vel_000007.raw", dtype=np.float32).reshape(lz, ly, lx, 3)
+    assert np.array_equal(v[..., 1], -rho)  # velprint(1:3,i,j,k): components innermost
+    x = (tmp_path / "out_vel_000007.xdmf").read_text()
+    assert 'Dimensions="3 4 5"' in x and 'Dimensions="3 4 5 3"' in x and "out_vel_000007.raw" in x
+
+
+@pytest.mark.parametrize("bad", [dict(lattice=15), dict(highorder=1, lattice=19), dict(densratio=1),
+                                 dict(lx=0), dict(storage="f8"), dict(visc1=-1.0)])
+def test_create_rejects_invalid_parameters_before_device_work(bad):
+    kw = dict(lx=8, ly=8, lz=8, lattice=27)
+    kw.update(bad)
+    if kw.get("storage") == "f8":
+        p = capi.Params(**{k: v for k, v in kw.items() if k != "storage"}).to_c()
+        p.storage = 9
+    else:
+        p = capi.Params(**kw).to_c()
+    h = C.c_void_p()
+    rc = capi.load().lbf_create(C.byref(p), C.byref(h))
+    assert rc in (-1, -5) and not h
+    assert capi.last_error()

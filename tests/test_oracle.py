@@ -1,0 +1,98 @@
+"""The CPU oracle against what pins it: the reference's Minv_mrt table, the
+reference's analytic Taylor-Green check (statistics.f90:918-956), and the
+invariants of the scheme.  No GPU."""
+import os
+
+import numpy as np
+import pytest
+
+from cases import make_case, rel_l2, run_oracle
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_minv_table_matches_reference_table():
+    ref = np.load(os.path.join(GOLDEN, "minv_mrt.npy"))  # parsed from vars_module.f90:360-521
+    assert np.abs(O.minv_table() - ref).max() < 1e-15
+
+
+def _tg(L, u0, nu, steps, chunk, prec="f64"):
+    p = dict(lx=L, ly=L, lz=L, pbc_x=1, pbc_y=1, pbc_z=1, lattice=19, highorder=0, twocomp=0, densratio=0,
+             obstacles=0, visc1=nu)
+    o = O.Oracle(p, prec)
+    o.set_isfluid(np.ones((L, L, L), np.int8))
+    o.set_fields(O.ic_taylor_green(L, L, L, u0))
+    t, e = [], []
+    for _ in range(steps // chunk + 1):
+        _, vel, _ = o.get_print()
+        t.append(o.nstep)
+        e.append(0.5 * np.mean((vel ** 2).sum(0)))
+        o.step(chunk)
+    return np.array(t), np.array(e), o
+
+
+def test_taylor_green_viscous_decay():
+    """statistics.f90:918-956: E/E0 ~ exp(-6 nu k^2 t); fit nu in the linear regime."""
+    L, nu = 24, 0.01
+    t, e, _ = _tg(L, 5e-4, nu, 300, 50)
+    k = 2 * np.pi / L
+    sel = t >= 50  # after the initial non-equilibrium transient of the regularised start
+    slope = np.polyfit(t[sel], np.log(e[sel] / e[0]), 1)[0]
+    nu_fit = -slope / (6 * k * k)
+    assert abs(nu_fit / nu - 1) < 0.03, nu_fit
+
+
+def test_one_component_conserves_mass_and_momentum():
+    _, _, o = _tg(16, 0.05, 0.02, 60, 60)
+    h0 = O.ic_taylor_green(16, 16, 16, 0.05)
+    h, _, _ = o.get_fields()
+    assert abs(h[0].sum() - h0[0].sum()) < 1e-12
+    for f in (1, 2, 3):
+        assert abs(h[f].sum() - h0[f].sum()) < 1e-12
+
+
+def test_rest_state_is_stationary():
+    for name in ("q27ho_2c_dr", "q19_2c", "tg_q19"):
+        p, isf, m, phi = make_case(name)
+        d = p.oracle_dict()
+        d.update(fx=0.0, fy=0.0, fz=0.0)  # no body force: the rest state must stay at rest
+        o = O.Oracle(d, "f64")
+        o.set_isfluid(isf)
+        z = np.zeros_like(m)
+        ph = None if phi is None else np.full(phi.shape, 0.3)
+        o.set_fields(z, ph)
+        o.step(5)
+        h, phi2, _ = o.get_fields()
+        assert np.abs(h).max() < 1e-14
+        if ph is not None:
+            assert np.abs(phi2 - 0.3).max() < 1e-14
+
+
+@pytest.mark.parametrize("name", ["q27ho_2c_dr", "obs_q19_1c"])
+def test_single_precision_build_tracks_double(name):
+    a = run_oracle(name, 10, "f64")
+    b = run_oracle(name, 10, "f32")
+    p, isf, _, _ = make_case(name)
+    fl = np.abs(isf) == 1
+    ha, pa, _ = a.get_fields()
+    hb, pb, _ = b.get_fields()
+    assert rel_l2(hb, ha, fl) < 1e-5
+    if p.twocomponent:
+        assert rel_l2(pb, pa, fl) < 1e-6
+
+
+def test_prime_wetting_copies_donor_phi():
+    """integrator_module.f90:186-190 runs the wetting before the loop with aux = 0:
+    every updated ghost equals its donor's phi (gradient terms vanish)."""
+    p, isf, m, phi = make_case("obs_q27ho_2c_dr")
+    o = O.Oracle(p.oracle_dict(), "f64")
+    o.set_isfluid(isf)
+    o.set_fields(m, phi)
+    o.step(0)
+    a, _ = o.get_phi_buffers()
+    solid = (isf == 0) & np.isfinite(phi)
+    changed = solid & (np.abs(a - phi) > 0)
+    assert changed.sum() > 0
+    vals = a[changed]
+    assert np.all((vals >= 0) & (vals <= 1))
