@@ -207,6 +207,63 @@ int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run);
 int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
                        const float* press);
 
+/* ---------------------------------------------------------------------------
+ * Batched solve server (no counterpart in the reference, which runs one box
+ * per process).  Independent solves of uneven box sizes are submitted as they
+ * arrive; a solve is admitted when its resident device bytes fit the memory
+ * budget (first in, first out), its fields stay in device memory until it
+ * finishes, and every time step of all resident solves of one kernel class
+ * (lattice, HIGHORDER, TWOCOMPONENT, storage) is ONE kernel launch over a
+ * work list of (solve, tile, z segment) items, replayed as a captured CUDA
+ * graph of `chunk` steps.  Solves that arrive while others run are admitted
+ * at the next chunk boundary.  A solve's result does not depend on what else
+ * is resident.  Each call must come from one host thread at a time.
+ * ------------------------------------------------------------------------- */
+typedef struct lbf_server lbf_server;
+
+typedef struct lbf_server_config {
+    long long mem_budget; /* device bytes resident solves may hold; <= 0: 80% of the free memory */
+    int max_active;       /* resident solves at most; <= 0: no limit */
+    int chunk;            /* steps per graph replay (even; <= 0: 32) */
+    int use_graph;        /* 1: replay captured CUDA graphs; 0: launch every step */
+} lbf_server_config;
+
+enum { LBF_SOLVE_QUEUED = 0, LBF_SOLVE_ACTIVE = 1, LBF_SOLVE_DONE = 2, LBF_SOLVE_FAILED = 3, LBF_SOLVE_CANCELLED = 4 };
+
+typedef struct lbf_solve_info {
+    int state;            /* LBF_SOLVE_* */
+    long long steps_done;
+    long long nsteps;
+    long long device_bytes;
+    /* CLOCK_MONOTONIC seconds (Python: time.monotonic()); 0 while not reached */
+    double t_submit, t_admit, t_done;
+} lbf_solve_info;
+
+int lbf_server_create(const lbf_server_config* cfg, lbf_server** out);
+/* waits for the device, frees every resident solve and record */
+int lbf_server_destroy(lbf_server* s);
+/* Queues one solve of nsteps steps of the box p describes (p->obstacles: isfluid
+ * as for lbf_set_isfluid, else NULL) from the fields mom10/phi of lbf_set_fields
+ * in dtype; the inputs are copied, the caller may free them on return.  A solve
+ * whose resident bytes exceed the budget is rejected with LBF_E_NOMEM. */
+int lbf_server_submit(lbf_server* s, const lbf_params* p, const int8_t* isfluid, const void* mom10, const void* phi,
+                      int dtype, long long nsteps, long long* id);
+/* Admits queued solves that fit, advances the resident ones by up to
+ * max_chunks chunks (each ends with a device synchronisation), and retires
+ * finished solves (their fields are copied to host memory and their device
+ * memory is released, which may admit more).  Returns after max_chunks chunks
+ * or when nothing is resident; *active and *queued (either may be NULL) give
+ * the counts on return. */
+int lbf_server_run(lbf_server* s, int max_chunks, int* active, int* queued);
+int lbf_server_poll(lbf_server* s, long long id, lbf_solve_info* info);
+/* Copies a finished solve's mom10 and phi (either may be NULL) in the dtype it
+ * was submitted with and forgets it; LBF_E_STATE until it is done. */
+int lbf_server_fetch(lbf_server* s, long long id, void* mom10, void* phi);
+/* Drops a queued or resident solve; its device memory is released at once. */
+int lbf_server_cancel(lbf_server* s, long long id);
+/* Device bytes a solve of these parameters holds while resident. */
+long long lbf_server_solve_bytes(const lbf_params* p);
+
 #ifdef __cplusplus
 }
 #endif

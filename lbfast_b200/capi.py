@@ -25,8 +25,10 @@ EXPORTED = (
     "lbf_version", "lbf_last_error", "lbf_create", "lbf_destroy", "lbf_set_stream", "lbf_set_isfluid",
     "lbf_set_fields", "lbf_step", "lbf_sync", "lbf_get_step", "lbf_get_fields", "lbf_get_print_fields",
     "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
-    "lbf_write_raw_xdmf",
+    "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
+    "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel",
 )
+SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
 
 class LbfParams(C.Structure):
@@ -40,6 +42,16 @@ class LbfParams(C.Structure):
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
         ("printphi", C.c_int), ("zseg", C.c_int),
     ]
+
+
+class LbfServerConfig(C.Structure):
+    _fields_ = [("mem_budget", C.c_longlong), ("max_active", C.c_int), ("chunk", C.c_int), ("use_graph", C.c_int)]
+
+
+class LbfSolveInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("steps_done", C.c_longlong), ("nsteps", C.c_longlong),
+                ("device_bytes", C.c_longlong), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double)]
 
 
 class LbfError(RuntimeError):
@@ -79,6 +91,15 @@ def load() -> C.CDLL:
     lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
     lib.lbf_ic_droplet.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
     lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    lib.lbf_server_create.argtypes = [P(LbfServerConfig), P(vp)]
+    lib.lbf_server_destroy.argtypes = [vp]
+    lib.lbf_server_submit.argtypes = [vp, P(LbfParams), i8p, vp, vp, C.c_int, C.c_longlong, P(C.c_longlong)]
+    lib.lbf_server_run.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int)]
+    lib.lbf_server_poll.argtypes = [vp, C.c_longlong, P(LbfSolveInfo)]
+    lib.lbf_server_fetch.argtypes = [vp, C.c_longlong, vp, vp]
+    lib.lbf_server_cancel.argtypes = [vp, C.c_longlong]
+    lib.lbf_server_solve_bytes.argtypes = [P(LbfParams)]
+    lib.lbf_server_solve_bytes.restype = C.c_longlong
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int if name != "lbf_version" else C.c_char_p
     _lib = lib
@@ -230,6 +251,85 @@ class Solver:
         out = np.zeros(5, dtype=np.float64)
         check(self.lib.lbf_reduce(self.h, _ptr(out, C.c_double)))
         return out
+
+
+class Server:
+    """Batched solve server (lbf_server_* of the C ABI): solves of uneven box
+    sizes are submitted as they arrive, admitted first in, first out against a
+    device-memory budget, and advanced together, one kernel launch per time
+    step for all resident solves of a kernel class, in CUDA-graph chunks."""
+
+    def __init__(self, mem_budget: int = 0, max_active: int = 0, chunk: int = 32, use_graph: bool = True):
+        self.lib = load()
+        cfg = LbfServerConfig(int(mem_budget), int(max_active), int(chunk), int(bool(use_graph)))
+        self.s = C.c_void_p()
+        check(self.lib.lbf_server_create(C.byref(cfg), C.byref(self.s)))
+        self._meta: dict[int, tuple] = {}
+
+    def close(self) -> None:
+        if self.s:
+            check(self.lib.lbf_server_destroy(self.s))
+            self.s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def solve_bytes(params: Params) -> int:
+        return int(load().lbf_server_solve_bytes(C.byref(params.to_c())))
+
+    def submit(self, params: Params, mom10: np.ndarray, phi: np.ndarray | None = None, nsteps: int = 1,
+               isf: np.ndarray | None = None) -> int:
+        dt = LBF_F64 if mom10.dtype == np.float64 else LBF_F32
+        npdt = np.float64 if dt == LBF_F64 else np.float32
+        shape = params.shape
+        m = np.ascontiguousarray(mom10, dtype=npdt).reshape((10,) + shape)
+        p = None if phi is None else np.ascontiguousarray(phi, dtype=npdt).reshape(shape)
+        i = None if isf is None else np.ascontiguousarray(isf, dtype=np.int8).reshape(shape)
+        sid = C.c_longlong()
+        check(self.lib.lbf_server_submit(self.s, C.byref(params.to_c()), _ptr(i, C.c_int8), _ptr(m), _ptr(p), dt,
+                                         int(nsteps), C.byref(sid)))
+        self._meta[sid.value] = (shape, npdt, bool(params.twocomponent))
+        return sid.value
+
+    def run(self, max_chunks: int = 1) -> tuple[int, int]:
+        """Advance up to max_chunks chunks; returns (resident, queued) solves."""
+        a, q = C.c_int(), C.c_int()
+        check(self.lib.lbf_server_run(self.s, int(max_chunks), C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def drain(self) -> None:
+        while self.run(1 << 20) != (0, 0):
+            pass
+
+    def poll(self, sid: int) -> dict:
+        info = LbfSolveInfo()
+        check(self.lib.lbf_server_poll(self.s, int(sid), C.byref(info)))
+        return {"state": SOLVE_STATE[info.state], "steps_done": info.steps_done, "nsteps": info.nsteps,
+                "device_bytes": info.device_bytes, "t_submit": info.t_submit, "t_admit": info.t_admit,
+                "t_done": info.t_done}
+
+    def fetch(self, sid: int):
+        """(mom10, phi) of a finished solve in the dtype it was submitted with."""
+        shape, npdt, tc = self._meta[sid]
+        m = np.empty((10,) + shape, dtype=npdt)
+        p = np.empty(shape, dtype=npdt) if tc else None
+        check(self.lib.lbf_server_fetch(self.s, int(sid), _ptr(m), _ptr(p)))
+        del self._meta[sid]
+        return m, p
+
+    def cancel(self, sid: int) -> None:
+        check(self.lib.lbf_server_cancel(self.s, int(sid)))
+        self._meta.pop(sid, None)
 
 
 # ---- host-side set-up helpers (C++ behind the C ABI) ----

@@ -18,6 +18,7 @@
 
 #include "../../include/lbfast_gpu.h"
 #include "lbf_internal.h"
+#include "lbf_handle.h"
 
 namespace {
 
@@ -51,44 +52,7 @@ namespace lbf {
 void record_error(const char* msg) { g_last_error = msg; }
 }  // namespace lbf
 
-struct lbf_handle {
-    lbf_params p;
-    int nx = 0, ny = 0, nz = 0;
-    long long N = 0;
-    int storage = 0;
-    size_t esz = 4, psz = 4;
-    bool tc = false, dr = false, obs = false;
-    double omega = 0, beta = 0, kapp = 0, sharp_c = 0;
-    double scale[lbf::NSCALE_H];
-    void* mom[2] = {nullptr, nullptr};
-    void* uold[2] = {nullptr, nullptr};
-    void* phi[2] = {nullptr, nullptr};
-    float* pres[2] = {nullptr, nullptr};  // P in FP32 when the other moments are 16-bit
-    int8_t* isf = nullptr;
-    bool isf_set = false;
-    int cur = 0;
-    long long step = 0;
-    bool fields_set = false, primed = false;
-    bool u_valid = false;  // uold[cur] holds the post-force velocity of the last step
-    // wetting
-    int nwet = 0;
-    long long* wet_s = nullptr;
-    int* wet_donor = nullptr;
-    int* wet_flag = nullptr;
-    double* wet_wn = nullptr;
-    int* wet_shift = nullptr;
-    void* wetW[2] = {nullptr, nullptr};
-    int wet_pending = -1;         // W buffer holding ghost values not yet written
-    int wet_pending_target = -1;  // phi buffer they belong to
-    double cot_theta = 0;
-    cudaStream_t stream = nullptr;
-    int* d_err = nullptr;
-    double* d_red = nullptr;
-    void* staging = nullptr;
-    size_t staging_bytes = 0;
-    lbf::StepLauncher launcher = nullptr;
-    int zseg = 0;
-};
+
 
 namespace {
 
@@ -495,36 +459,14 @@ int lbf_step(lbf_handle* h, int nsteps) {
         if (rc) return rc;
     }
     lbf::StepArgs a;
-    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
-    a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
-    a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg;
-    a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
-    a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
-    a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;
-    a.fx = h->p.fx; a.fy = h->p.fy; a.fz = h->p.fz;
-    for (int i = 0; i < lbf::NSCALE_H; ++i) a.scale[i] = h->scale[i];
-    a.isf = h->obs ? h->isf : nullptr;
-    a.err = h->d_err;
-    a.pres_in = nullptr;
-    a.pres_out = nullptr;
     for (int s = 0; s < nsteps; ++s) {
-        const int in = h->cur, out = 1 - h->cur;
-        int rc = launch_wet(h, in, out, false);
+        int rc = launch_wet(h, h->cur, 1 - h->cur, false);
         if (rc) return rc;
-        a.min = h->mom[in];
-        a.mout = h->mom[out];
-        a.uin = h->uold[in];
-        a.uout = h->uold[out];
-        a.pin = h->phi[in];
-        a.pout = h->phi[out];
-        a.pres_in = h->pres[in];
-        a.pres_out = h->pres[out];
-        a.write_u = (h->dr || s == nsteps - 1) ? 1 : 0;
+        const bool write_u = h->dr || s == nsteps - 1;
+        lbf::handle_step_args(h, a, write_u);
         cudaError_t e = h->launcher(a, h->stream);
         if (e != cudaSuccess) return fail(LBF_E_CUDA, "step kernel launch: %s", cudaGetErrorString(e));
-        h->cur = out;
-        h->step++;
-        h->u_valid = a.write_u != 0;
+        lbf::handle_advance(h, write_u);
     }
     return LBF_OK;
 }
@@ -657,3 +599,60 @@ int lbf_reduce(lbf_handle* h, double out[5]) {
 }
 
 }  // extern "C"
+
+namespace lbf {
+
+int handle_prime(lbf_handle* h) { return h->primed ? LBF_OK : prime(h); }
+
+void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u) {
+    const int in = h->cur, out = 1 - h->cur;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+    a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
+    a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg;
+    a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
+    a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
+    a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;
+    a.fx = h->p.fx; a.fy = h->p.fy; a.fz = h->p.fz;
+    for (int i = 0; i < NSCALE_H; ++i) a.scale[i] = h->scale[i];
+    a.isf = h->obs ? h->isf : nullptr;
+    a.err = h->d_err;
+    a.min = h->mom[in];
+    a.mout = h->mom[out];
+    a.uin = h->uold[in];
+    a.uout = h->uold[out];
+    a.pin = h->phi[in];
+    a.pout = h->phi[out];
+    a.pres_in = h->pres[in];
+    a.pres_out = h->pres[out];
+    a.write_u = write_u ? 1 : 0;
+}
+
+void handle_advance(lbf_handle* h, bool wrote_u) {
+    h->cur = 1 - h->cur;
+    h->step++;
+    h->u_valid = wrote_u;
+}
+
+size_t handle_bytes(const lbf_params* p) {
+    const long long N = (long long)p->lx * p->ly * p->lz;
+    const size_t esz = storage_bytes(p->storage), psz = phi_bytes(p->storage);
+    const bool half = p->storage == LBF_STORE_F16 || p->storage == LBF_STORE_BF16;
+    size_t b = 2 * (13 * N * esz);
+    if (p->twocomponent) b += 2 * N * psz;
+    if (half) b += 2 * N * sizeof(float);
+    if (p->obstacles) b += N;
+    return b;
+}
+
+int handle_pre_step(lbf_handle* h) { return launch_wet(h, h->cur, 1 - h->cur, false); }
+
+bool handle_steady(const lbf_handle* h) { return !(h->tc && h->obs && h->nwet > 0) || h->wet_pending >= 0; }
+
+void handle_release_staging(lbf_handle* h) {
+    if (!h->staging) return;
+    cudaFree(h->staging);
+    h->staging = nullptr;
+    h->staging_bytes = 0;
+}
+
+}  // namespace lbf

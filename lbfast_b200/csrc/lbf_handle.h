@@ -1,0 +1,64 @@
+// lbf_handle.h -- the device state behind an lbf_handle and the internal
+// hooks the batched server (lbf_server.cu) shares with the single-box C ABI
+// (lbf_capi.cu).  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/lbfast_gpu.h"
+#include "lbf_internal.h"
+
+struct lbf_handle {
+    lbf_params p;
+    int nx = 0, ny = 0, nz = 0;
+    long long N = 0;
+    int storage = 0;
+    size_t esz = 4, psz = 4;
+    bool tc = false, dr = false, obs = false;
+    double omega = 0, beta = 0, kapp = 0, sharp_c = 0;
+    double scale[lbf::NSCALE_H];
+    void* mom[2] = {nullptr, nullptr};
+    void* uold[2] = {nullptr, nullptr};
+    void* phi[2] = {nullptr, nullptr};
+    float* pres[2] = {nullptr, nullptr};  // P in FP32 when the other moments are 16-bit
+    int8_t* isf = nullptr;
+    bool isf_set = false;
+    int cur = 0;
+    long long step = 0;
+    bool fields_set = false, primed = false;
+    bool u_valid = false;  // uold[cur] holds the post-force velocity of the last step
+    // wetting
+    int nwet = 0;
+    long long* wet_s = nullptr;
+    int* wet_donor = nullptr;
+    int* wet_flag = nullptr;
+    double* wet_wn = nullptr;
+    int* wet_shift = nullptr;
+    void* wetW[2] = {nullptr, nullptr};
+    int wet_pending = -1;         // W buffer holding ghost values not yet written
+    int wet_pending_target = -1;  // phi buffer they belong to
+    double cot_theta = 0;
+    cudaStream_t stream = nullptr;
+    int* d_err = nullptr;
+    double* d_red = nullptr;
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    lbf::StepLauncher launcher = nullptr;
+    int zseg = 0;
+};
+
+namespace lbf {
+// integrator pre-loop work (wetting) of a freshly filled handle
+int handle_prime(lbf_handle* h);
+// launch arguments of the next step of h (its current time level)
+void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u);
+// bookkeeping after one step of h was launched
+void handle_advance(lbf_handle* h, bool wrote_u);
+// device bytes lbf_create allocates for these parameters
+size_t handle_bytes(const lbf_params* p);
+// per-step work of h launched before its step kernel (wetting ghost update)
+int handle_pre_step(lbf_handle* h);
+// true when the per-step work of h repeats with period two (replayable)
+bool handle_steady(const lbf_handle* h);
+// frees the host<->device staging buffer (reallocated on the next transfer)
+void handle_release_staging(lbf_handle* h);
+}  // namespace lbf

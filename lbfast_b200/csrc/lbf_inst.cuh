@@ -7,18 +7,10 @@
 
 namespace lbf {
 
-template <int LAT, bool HO, bool TC, typename S, typename R>
-cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
+static_assert(TX == STEP_TILE_X && TY == STEP_TILE_Y, "host tile constants must match the kernel's");
+
+template <typename S, typename R> void make_params(const StepArgs& a, StepParams<S, R>& p) {
     using SP = typename PhiStore<S>::type;
-    static bool attr_set = false;
-    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    StepParams<S, R> p;
     p.nx = a.nx; p.ny = a.ny; p.nz = a.nz;
     p.pbx = a.pbx; p.pby = a.pby; p.pbz = a.pbz;
     p.plane = (long long)a.nx * a.ny;
@@ -43,9 +35,56 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     p.pres_out = a.pres_out;
     p.isf = a.isf;
     p.err = a.err;
+}
+
+template <int LAT, bool HO, bool TC, typename S, typename R>
+cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
+    static bool attr_set = false;
+    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    StepParams<S, R> p;
+    make_params(a, p);
     dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zseg - 1) / a.zseg);
     stream_kernel<LAT, HO, TC, S, R><<<grid, NT, smem, st>>>(p);
     return cudaGetLastError();
+}
+
+// One launch advancing many boxes of one kernel class: d_boxes holds one
+// StepParams per box, d_work one (box, tile x, tile y, z segment) per CTA.
+template <int LAT, bool HO, bool TC, typename S, typename R>
+cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st) {
+    static bool attr_set = false;
+    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (nwork <= 0) return cudaSuccess;
+    stream_kernel_batched<LAT, HO, TC, S, R>
+        <<<nwork, NT, smem, st>>>(static_cast<const StepParams<S, R>*>(d_boxes), d_work);
+    return cudaGetLastError();
+}
+
+template <typename S, typename R> void fill_params(const StepArgs& a, void* dst) {
+    make_params(a, *static_cast<StepParams<S, R>*>(dst));
+}
+
+template <typename S, typename R> BatchOps batch_table(int lat, int ho, int tc) {
+    BatchOps o;
+    o.params_bytes = sizeof(StepParams<S, R>);
+    o.fill = &fill_params<S, R>;
+    o.launch = nullptr;
+    if (lat == 19 && !ho) o.launch = tc ? &launch_stream_batched<19, false, true, S, R> : &launch_stream_batched<19, false, false, S, R>;
+    if (lat == 27 && ho) o.launch = tc ? &launch_stream_batched<27, true, true, S, R> : &launch_stream_batched<27, true, false, S, R>;
+    if (lat == 27 && !ho) o.launch = tc ? &launch_stream_batched<27, false, true, S, R> : &launch_stream_batched<27, false, false, S, R>;
+    return o;
 }
 
 template <typename S, typename R> StepLauncher step_table(int lat, int ho, int tc) {

@@ -34,6 +34,22 @@ StepLauncher step_launcher_f16(int lat, int ho, int tc);
 StepLauncher step_launcher_bf16(int lat, int ho, int tc);
 StepLauncher step_launcher_f64(int lat, int ho, int tc);
 
+// Batched step of many boxes of one kernel class (lattice, HIGHORDER,
+// TWOCOMPONENT, storage): fill writes the device-format parameters of one box
+// (params_bytes bytes) from its StepArgs; launch runs one CTA per work item
+// (int4: box, tile x, tile y, z segment).
+struct BatchOps {
+    size_t params_bytes;
+    void (*fill)(const StepArgs&, void*);
+    cudaError_t (*launch)(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st);
+};
+BatchOps batch_ops_f32(int lat, int ho, int tc);
+BatchOps batch_ops_f16(int lat, int ho, int tc);
+BatchOps batch_ops_bf16(int lat, int ho, int tc);
+BatchOps batch_ops_f64(int lat, int ho, int tc);
+// CTA tile of the step kernel (x, y) in nodes
+constexpr int STEP_TILE_X = 32, STEP_TILE_Y = 8;
+
 // wetting tables (solid nodes whose ghost phi the reference updates)
 struct WetArgs {
     int n;                    // entries

@@ -57,8 +57,9 @@ template <int LAT, bool TC, typename S, typename R> constexpr size_t stream_smem
     return b;
 }
 
+// One CTA's share of a time step: tile (bx, by) of the box, z segment bz.
 template <int LAT, bool HO, bool TC, typename S, typename R>
-__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(const StepParams<S, R> p) {
+__device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int bz) {
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
     using CP = Codec<SP>;
@@ -72,8 +73,8 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(co
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
-    const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY;
-    const int z0 = blockIdx.z * p.zseg;
+    const int X0 = bx * TX, Y0 = by * TY;
+    const int z0 = bz * p.zseg;
     const int z1 = min(z0 + p.zseg, p.nz);
     const long long N = p.N, plane = p.plane;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
@@ -622,6 +623,26 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(co
         cp_async_wait_all();
         __syncthreads();
     }
+}
+
+// Single box: one CTA per (tile x, tile y, z segment).
+template <int LAT, bool HO, bool TC, typename S, typename R>
+__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(const StepParams<S, R> p) {
+    step_body<LAT, HO, TC, S, R>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many boxes in one launch: CTA i advances box work[i].x, tile (work[i].y,
+// work[i].z), z segment work[i].w, with that box's own parameters and fields.
+// Each node's arithmetic is the same as in stream_kernel, so a box gives the
+// same bits alone and in a batch.
+template <int LAT, bool HO, bool TC, typename S, typename R>
+__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2))
+    stream_kernel_batched(const StepParams<S, R>* __restrict__ boxes, const int4* __restrict__ work) {
+    __shared__ StepParams<S, R> sp;
+    const int4 w = work[blockIdx.x];
+    if (threadIdx.x == 0) sp = boxes[w.x];
+    __syncthreads();
+    step_body<LAT, HO, TC, S, R>(sp, w.y, w.z, w.w);
 }
 
 }  // namespace lbf
