@@ -201,6 +201,130 @@ def run_ours(args, rank, local, world):
             "finite": ok}
 
 
+# ---- serving: an ensemble of droplet solves of uneven box sizes ----------
+
+SERVE_EDGES = (32, 48, 64, 96, 128)
+
+
+def p2_droplet(edge: int, eps: float, ratio: float, sigma: float = 0.03, width: float = 5.0, _cache={}):
+    """Droplet of radius R = edge/4 at the box centre with the surface
+    r_s(theta) = R (1 + eps P2(cos theta)), the fcut_tanh profile and the
+    Laplace pressure of the reference's droplet set-up
+    (init_conditions_module.f90:394-426); fluids at rest.  float32 fields."""
+    import numpy as np
+    if edge not in _cache:
+        c = edge / 2
+        x = np.arange(1, edge + 1) - c
+        z, y, xx = np.meshgrid(x, x, x, indexing="ij")
+        r = np.sqrt(xx * xx + y * y + z * z)
+        ct = np.divide(z, r, out=np.zeros_like(r), where=r > 0)
+        _cache[edge] = (r.astype(np.float32), (0.5 * (3 * ct * ct - 1)).astype(np.float32))
+    r, p2 = _cache[edge]
+    R = edge / 4
+    rs = R * (1 + eps * p2)
+    phi = 0.5 * (1 - np.tanh((r - rs) / (0.5 * width)))
+    rhophi = ratio * phi + (1 - phi)
+    m = np.zeros((10, edge, edge, edge), np.float32)
+    m[0] = phi * (2 * sigma) / R / (rhophi / 3)
+    return m, phi.astype(np.float32)
+
+
+def serving_jobs(n: int, seed: int = 7):
+    """n solves: edge uniform over SERVE_EDGES, eps ~ U[0.05, 0.15], density
+    ratio log-uniform over [10, 1000] (rho_b = 1); D3Q27 two-component
+    DENSRATIO, FP16 storage, sigma 0.03, nu 0.001, tau_diff 0.1, width 5."""
+    import numpy as np
+    import lbfast_b200 as lbf
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(n):
+        e = int(rng.choice(SERVE_EDGES))
+        eps = float(rng.uniform(0.05, 0.15))
+        ratio = float(np.exp(rng.uniform(np.log(10.0), np.log(1000.0))))
+        p = lbf.Params(lx=e, ly=e, lz=e, lattice=27, highorder=0, twocomponent=1, densratio=1, visc1=0.001,
+                       visc2=0.001, rho_r=ratio, rho_b=1.0, sigma=0.03, width=5.0, tau_diff=0.1, storage="f16")
+        m, phi = p2_droplet(e, eps, ratio)
+        jobs.append((p, m, phi))
+    return jobs
+
+
+def _drain(srv, jobs, nsteps):
+    ids = [srv.submit(p, m, phi, nsteps) for p, m, phi in jobs]
+    srv.drain()
+    return ids
+
+
+def run_serving(n: int, nsteps: int, seed: int = 7):
+    """Solves/s of the batched server against the same solves run one at a
+    time on the same engine (max_active = 1: same kernel, same graphs, no
+    batching), the saturated throughput (all submitted at once), and per-solve
+    latency under seeded Poisson arrivals at 1.5x the one-at-a-time rate."""
+    import numpy as np
+    import lbfast_b200 as lbf
+    jobs = serving_jobs(n, seed)
+    lups = sum(p.lx * p.ly * p.lz for p, _, _ in jobs) * nsteps
+    # warm-up: kernel attributes, graph machinery, allocator
+    with lbf.Server(chunk=32) as srv:
+        _drain(srv, jobs[:2], 64)
+    # one at a time
+    with lbf.Server(max_active=1, chunk=32) as srv:
+        t0 = time.monotonic()
+        ids = _drain(srv, jobs, nsteps)
+        t_seq = time.monotonic() - t0
+        svc = {}
+        for (p, _, _), i in zip(jobs, ids):
+            info = srv.poll(i)
+            svc.setdefault(p.lx, []).append(info["t_done"] - info["t_admit"])
+        seq_out = [srv.fetch(i) for i in ids]
+    # lattice updates per second of one solve running alone, by box edge
+    alone_mlups = {e: e ** 3 * nsteps / float(np.mean(v)) / 1e6 for e, v in sorted(svc.items())}
+    # batched, saturated
+    with lbf.Server(chunk=32) as srv:
+        t0 = time.monotonic()
+        ids = _drain(srv, jobs, nsteps)
+        t_bat = time.monotonic() - t0
+        peak_bytes = sum(srv.poll(i)["device_bytes"] for i in ids)
+        same = all(all(np.array_equal(a, b, equal_nan=True) for a, b in zip(srv.fetch(i), ref))
+                   for i, ref in zip(ids, seq_out))
+    del seq_out
+    # batched, open loop: Poisson arrivals at 1.5x the one-at-a-time rate
+    lam = 1.5 * n / t_seq
+    rng = np.random.default_rng(seed)
+    arrive = np.cumsum(rng.exponential(1.0 / lam, n))
+    lat = []
+    with lbf.Server(chunk=32) as srv:
+        t0 = time.monotonic()
+        nxt, pending = 0, {}
+        while nxt < n or pending:
+            now = time.monotonic() - t0
+            while nxt < n and arrive[nxt] <= now:
+                p, m, phi = jobs[nxt]
+                pending[srv.submit(p, m, phi, nsteps)] = t0 + arrive[nxt]
+                nxt += 1
+            active, queued = srv.run(1)
+            for sid in [i for i in pending if srv.poll(i)["state"] == "done"]:
+                lat.append(srv.poll(sid)["t_done"] - pending.pop(sid))
+                srv.fetch(sid)
+            if active == 0 and queued == 0 and nxt < n:
+                time.sleep(max(0.0, arrive[nxt] - (time.monotonic() - t0)))
+        t_open = time.monotonic() - t0
+    lat = np.sort(np.array(lat))
+    edges = {e: sum(1 for p, _, _ in jobs if p.lx == e) for e in SERVE_EDGES}
+    return {
+        "workload": f"{n} droplet solves x {nsteps} steps, edges {list(SERVE_EDGES)} (counts {edges}), "
+                    "R = edge/4 with a P2 shape perturbation eps ~ U[0.05,0.15], density ratio log-uniform "
+                    "[10,1000], D3Q27 two-component DENSRATIO, FP16 storage, nu 0.001, sigma 0.03, width 5, seed 7",
+        "solves_per_s": n / t_bat, "solves_per_s_one_at_a_time": n / t_seq, "speedup": t_seq / t_bat,
+        "mlups_batched": lups / t_bat / 1e6, "mlups_one_at_a_time": lups / t_seq / 1e6,
+        "mlups_alone_by_edge": alone_mlups,
+        "open_loop": {"arrival_rate_per_s": lam, "solves_per_s": n / t_open,
+                      "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                      "latency_max_s": float(lat[-1])},
+        "peak_resident_bytes": peak_bytes, "alone_equals_mix_bitwise": bool(same),
+        "timing": "host monotonic clock from first submit to last result on the host (fields copied back)",
+    }
+
+
 def cpu_baseline(storage: str, L: int, nsteps: int, threads: int):
     """The oracle (C restatement of the reference, FP32 build stand-in) on the
     host cores: `nsteps` steps of the same box."""
@@ -228,6 +352,8 @@ def main():
     ap.add_argument("--box", type=int, default=LBOX)
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-solves", type=int, default=40, help="solves of the serving measurement (0: skip)")
+    ap.add_argument("--serve-steps", type=int, default=3000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -270,6 +396,9 @@ def main():
         cpu = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{args.cpu_steps} steps of the same {args.box}^3 box ({dt:.1f} s), FP32 C restatement of "
                          f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
+    serving = None
+    if rank == 0 and world == 1 and args.serve_solves > 0:
+        serving = run_serving(args.serve_solves, args.serve_steps)
     if rank != 0:
         shutdown(world)
         return
@@ -283,7 +412,7 @@ def main():
                      "frac": r["achieved"] / peak, "traffic": traffic, "peak_source": peak_src,
                      "kernel": "lbf::stream_kernel<27,HO,TC>", "bytes_per_launch": B_LUP[args.storage] * args.box ** 3},
         "e2e": r["e2e"], "gpu_launches": args.steps, "clocks": r["clocks"], "cpu_baseline": cpu,
-        "finite": r["finite"],
+        "finite": r["finite"], "serving": serving,
     }
     print(json.dumps(line))
     shutdown(world)
