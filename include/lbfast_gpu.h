@@ -69,6 +69,10 @@ typedef struct lbf_params {
                                 (lb_cuda_boundary_module.f90:264,275) */
     int printphi;            /* PRINTPHI: `rho` output holds phi */
     int zseg;                /* planes per z segment of the kernel; 0 = automatic */
+    int tile_y;              /* rows of the kernel's 32-wide tile: 8 or 16 (FP64: 8 only); 0 = autotuned
+                                together with zseg (when zseg = 0) at the first lbf_step: each candidate
+                                (tile, zseg) is timed on the box itself, the fastest is kept and remembered
+                                for boxes of the same shape and class.  Results do not depend on either. */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;
@@ -114,6 +118,8 @@ int lbf_sync(lbf_handle* h);
 
 /* Number of steps done since lbf_set_fields. */
 int lbf_get_step(lbf_handle* h, long long* step);
+/* The kernel tile height and z segment in use (after the autotuner, if it ran). */
+int lbf_get_tuning(lbf_handle* h, int* tile_y, int* zseg);
 
 /* State a next step starts from: moments (10 x N), phi (N) and the velocity
  * after the force half-step of the last step (3 x N, the u_old of the next

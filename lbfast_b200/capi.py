@@ -26,7 +26,7 @@ EXPORTED = (
     "lbf_set_fields", "lbf_step", "lbf_sync", "lbf_get_step", "lbf_get_fields", "lbf_get_print_fields",
     "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
     "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
-    "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel",
+    "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning",
 )
 SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -40,7 +40,7 @@ class LbfParams(C.Structure):
         ("visc1", C.c_double), ("visc2", C.c_double), ("rho_r", C.c_double), ("rho_b", C.c_double),
         ("sigma", C.c_double), ("width", C.c_double), ("tau_diff", C.c_double),
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
-        ("printphi", C.c_int), ("zseg", C.c_int),
+        ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int),
     ]
 
 
@@ -84,6 +84,7 @@ def load() -> C.CDLL:
     lib.lbf_sync.argtypes = [vp]
     lib.lbf_get_step.argtypes = [vp, P(C.c_longlong)]
     lib.lbf_get_fields.argtypes = [vp, vp, vp, vp, C.c_int]
+    lib.lbf_get_tuning.argtypes = [vp, P(C.c_int), P(C.c_int)]
     lib.lbf_get_print_fields.argtypes = [vp, fp, fp, fp]
     lib.lbf_reduce.argtypes = [vp, dp]
     lib.lbf_mark_isfluid.argtypes = [C.c_int] * 8 + [i8p, i8p]
@@ -153,6 +154,7 @@ class Params:
     wettab_r: float = 90.0
     printphi: int = 0
     zseg: int = 0
+    tile_y: int = 0
 
     def to_c(self) -> LbfParams:
         p = LbfParams()
@@ -229,6 +231,13 @@ class Solver:
         s = C.c_longlong()
         check(self.lib.lbf_get_step(self.h, C.byref(s)))
         return s.value
+
+    @property
+    def tuning(self) -> tuple[int, int]:
+        """(tile rows, z segment) of the step kernel in use."""
+        ty, zs = C.c_int(), C.c_int()
+        check(self.lib.lbf_get_tuning(self.h, C.byref(ty), C.byref(zs)))
+        return ty.value, zs.value
 
     def get_fields(self, dtype=np.float64):
         dt = LBF_F64 if dtype == np.float64 else LBF_F32

@@ -13,6 +13,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -86,15 +88,104 @@ void free_all(lbf_handle* h) {
     cudaFree(h->staging);
 }
 
-// automatic z segment: enough CTAs for a few waves on 148 SMs, segments of at
-// least 8 planes so the pipeline fill (5 planes) stays a small overhead
-int auto_zseg(int nx, int ny, int nz) {
-    long long cols = (long long)((nx + 31) / 32) * ((ny + 7) / 8);
-    long long target = 148LL * 2 * 4;
+// automatic z segment: enough CTAs for about four waves on 148 SMs (two CTAs
+// of 8 rows or one of 16 rows per SM), segments of at least 8 planes so the
+// pipeline fill (5 planes) stays a small overhead
+int auto_zseg(int nx, int ny, int nz, int tile_y) {
+    long long cols = (long long)((nx + 31) / 32) * ((ny + tile_y - 1) / tile_y);
+    long long target = 148LL * 4 * (tile_y == 8 ? 2 : 1);
     int nseg = (int)std::max<long long>(1, (target + cols - 1) / cols);
     int zseg = (nz + nseg - 1) / nseg;
     zseg = std::max(zseg, std::min(nz, 8));
     return zseg;
+}
+
+// ---- autotuner of the tile height and z segment ----
+// Every candidate launch steps the current time level into the other buffer
+// set, which the next real step overwrites, so timing on the box's own fields
+// leaves its state unchanged (wetting, which changes host-side state, is not
+// part of a trial).  The winner is remembered per box shape and class.
+struct TuneKey {
+    int v[12];
+    bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 12, o.v, o.v + 12); }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune_cache;
+
+TuneKey tune_key(const lbf_handle* h) {
+    const lbf_params& p = h->p;
+    return TuneKey{{p.storage, p.lattice, p.highorder, p.twocomponent, p.densratio, p.obstacles, p.lx, p.ly, p.lz,
+                    p.pbc_x * 4 + p.pbc_y * 2 + p.pbc_z, p.zseg, 0}};
+}
+
+int autotune(lbf_handle* h) {
+    h->tuned = true;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(h->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return LBF_OK;  // keep the defaults inside a capture
+    const TuneKey key = tune_key(h);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            h->tile_y = it->second.first;
+            h->zseg = it->second.second;
+            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, h->tile_y);
+            return LBF_OK;
+        }
+    }
+    std::vector<std::pair<int, int>> cand;
+    for (int ty : {8, 16}) {
+        if (!lbf::tile_available(h->storage, ty)) continue;
+        std::vector<int> zs;
+        if (h->p.zseg > 0) {
+            zs.push_back(std::min(h->p.zseg, h->nz));
+        } else {
+            const int za = auto_zseg(h->nx, h->ny, h->nz, ty), lo = std::min(h->nz, 8);
+            for (int z : {za, std::max(lo, za / 2), std::min(h->nz, 2 * za), h->nz})
+                if (std::find(zs.begin(), zs.end(), z) == zs.end()) zs.push_back(z);
+        }
+        for (int z : zs) cand.emplace_back(ty, z);
+    }
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    std::pair<int, int> pick(h->tile_y, h->zseg);
+    int rc = LBF_OK;
+    for (const auto& c : cand) {
+        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, c.first);
+        if (!L) continue;
+        lbf::StepArgs a;
+        const int zs0 = h->zseg;
+        h->zseg = c.second;
+        lbf::handle_step_args(h, a, h->dr);
+        h->zseg = zs0;
+        cudaError_t e = L(a, h->stream);  // warm-up (first use sets the kernel's shared-memory limit)
+        if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = L(a, h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            rc = fail(LBF_E_CUDA, "autotune launch: %s", cudaGetErrorString(e));
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    h->tile_y = pick.first;
+    h->zseg = pick.second;
+    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, h->tile_y);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = pick;
+    return LBF_OK;
 }
 
 // Pre-loop wetting of integrator_module.f90:186-190 / one launch per step.
@@ -218,17 +309,22 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
         h->cot_theta = std::fabs(s) < 1.0e-14 ? std::copysign(1.0e14, c) : c / s;
     }
     for (int i = 0; i < lbf::NSCALE_H; ++i) h->scale[i] = 1.0;
-    switch (p->storage) {
-        case LBF_STORE_F32: h->launcher = lbf::step_launcher_f32(p->lattice, p->highorder, p->twocomponent); break;
-        case LBF_STORE_F16: h->launcher = lbf::step_launcher_f16(p->lattice, p->highorder, p->twocomponent); break;
-        case LBF_STORE_BF16: h->launcher = lbf::step_launcher_bf16(p->lattice, p->highorder, p->twocomponent); break;
-        case LBF_STORE_F64: h->launcher = lbf::step_launcher_f64(p->lattice, p->highorder, p->twocomponent); break;
+    if (p->tile_y != 0 && p->tile_y != 8 && p->tile_y != 16) {
+        delete h;
+        return fail(LBF_E_ARG, "tile_y must be 0 (autotuned), 8 or 16");
     }
+    if (p->tile_y != 0 && !lbf::tile_available(p->storage, p->tile_y)) {
+        delete h;
+        return fail(LBF_E_UNSUPPORTED, "tile of %d rows not built for this storage", p->tile_y);
+    }
+    h->tile_y = p->tile_y ? p->tile_y : 8;
+    h->tuned = p->tile_y != 0;
+    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, p->twocomponent, h->tile_y);
     if (!h->launcher) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
     }
-    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : auto_zseg(h->nx, h->ny, h->nz);
+    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : auto_zseg(h->nx, h->ny, h->nz, h->tile_y);
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
         ok = ok && cudaMalloc(&h->mom[b], 10 * h->N * h->esz) == cudaSuccess;
@@ -458,6 +554,10 @@ int lbf_step(lbf_handle* h, int nsteps) {
         int rc = prime(h);
         if (rc) return rc;
     }
+    if (!h->tuned && nsteps > 0) {
+        int rc = autotune(h);
+        if (rc) return rc;
+    }
     lbf::StepArgs a;
     for (int s = 0; s < nsteps; ++s) {
         int rc = launch_wet(h, h->cur, 1 - h->cur, false);
@@ -481,6 +581,13 @@ int lbf_sync(lbf_handle* h) {
 int lbf_get_step(lbf_handle* h, long long* step) {
     if (!h || !step) return fail(LBF_E_ARG, "lbf_get_step: null argument");
     *step = h->step;
+    return LBF_OK;
+}
+
+int lbf_get_tuning(lbf_handle* h, int* tile_y, int* zseg) {
+    if (!h || !tile_y || !zseg) return fail(LBF_E_ARG, "lbf_get_tuning: null argument");
+    *tile_y = h->tile_y;
+    *zseg = h->zseg;
     return LBF_OK;
 }
 

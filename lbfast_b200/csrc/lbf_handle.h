@@ -44,6 +44,8 @@ struct lbf_handle {
     size_t staging_bytes = 0;
     lbf::StepLauncher launcher = nullptr;
     int zseg = 0;
+    int tile_y = 8;      // rows of the kernel tile
+    bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
 };
 
 namespace lbf {

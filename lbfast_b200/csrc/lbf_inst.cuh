@@ -7,7 +7,7 @@
 
 namespace lbf {
 
-static_assert(TX == STEP_TILE_X && TY == STEP_TILE_Y, "host tile constants must match the kernel's");
+static_assert(TX == STEP_TILE_X, "host tile width must match the kernel's");
 
 template <typename S, typename R> void make_params(const StepArgs& a, StepParams<S, R>& p) {
     using SP = typename PhiStore<S>::type;
@@ -37,38 +37,38 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.err = a.err;
 }
 
-template <int LAT, bool HO, bool TC, typename S, typename R>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     static bool attr_set = false;
-    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
+    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     StepParams<S, R> p;
     make_params(a, p);
-    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zseg - 1) / a.zseg);
-    stream_kernel<LAT, HO, TC, S, R><<<grid, NT, smem, st>>>(p);
+    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
+    stream_kernel<LAT, HO, TC, S, R, TYV><<<grid, TX * TYV, smem, st>>>(p);
     return cudaGetLastError();
 }
 
 // One launch advancing many boxes of one kernel class: d_boxes holds one
 // StepParams per box, d_work one (box, tile x, tile y, z segment) per CTA.
-template <int LAT, bool HO, bool TC, typename S, typename R>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st) {
     static bool attr_set = false;
-    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R>();
+    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (nwork <= 0) return cudaSuccess;
-    stream_kernel_batched<LAT, HO, TC, S, R>
-        <<<nwork, NT, smem, st>>>(static_cast<const StepParams<S, R>*>(d_boxes), d_work);
+    stream_kernel_batched<LAT, HO, TC, S, R, TYV>
+        <<<nwork, TX * TYV, smem, st>>>(static_cast<const StepParams<S, R>*>(d_boxes), d_work);
     return cudaGetLastError();
 }
 
@@ -76,22 +76,29 @@ template <typename S, typename R> void fill_params(const StepArgs& a, void* dst)
     make_params(a, *static_cast<StepParams<S, R>*>(dst));
 }
 
-template <typename S, typename R> BatchOps batch_table(int lat, int ho, int tc) {
+// the five kernel classes of one storage type and tile height
+template <typename S, typename R, int TYV> StepLauncher step_table(int lat, int ho, int tc) {
+    if (lat == 19 && !ho) return tc ? &launch_stream<19, false, true, S, R, TYV> : &launch_stream<19, false, false, S, R, TYV>;
+    if (lat == 27 && ho) return tc ? &launch_stream<27, true, true, S, R, TYV> : &launch_stream<27, true, false, S, R, TYV>;
+    if (lat == 27 && !ho) return tc ? &launch_stream<27, false, true, S, R, TYV> : &launch_stream<27, false, false, S, R, TYV>;
+    return nullptr;
+}
+
+template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho, int tc) {
     BatchOps o;
     o.params_bytes = sizeof(StepParams<S, R>);
     o.fill = &fill_params<S, R>;
+    o.tile_y = TYV;
     o.launch = nullptr;
-    if (lat == 19 && !ho) o.launch = tc ? &launch_stream_batched<19, false, true, S, R> : &launch_stream_batched<19, false, false, S, R>;
-    if (lat == 27 && ho) o.launch = tc ? &launch_stream_batched<27, true, true, S, R> : &launch_stream_batched<27, true, false, S, R>;
-    if (lat == 27 && !ho) o.launch = tc ? &launch_stream_batched<27, false, true, S, R> : &launch_stream_batched<27, false, false, S, R>;
+    if (lat == 19 && !ho) o.launch = tc ? &launch_stream_batched<19, false, true, S, R, TYV> : &launch_stream_batched<19, false, false, S, R, TYV>;
+    if (lat == 27 && ho) o.launch = tc ? &launch_stream_batched<27, true, true, S, R, TYV> : &launch_stream_batched<27, true, false, S, R, TYV>;
+    if (lat == 27 && !ho) o.launch = tc ? &launch_stream_batched<27, false, true, S, R, TYV> : &launch_stream_batched<27, false, false, S, R, TYV>;
     return o;
 }
 
-template <typename S, typename R> StepLauncher step_table(int lat, int ho, int tc) {
-    if (lat == 19) return tc ? &launch_stream<19, false, true, S, R> : &launch_stream<19, false, false, S, R>;
-    if (lat != 27) return nullptr;
-    if (ho) return tc ? &launch_stream<27, true, true, S, R> : &launch_stream<27, true, false, S, R>;
-    return tc ? &launch_stream<27, false, true, S, R> : &launch_stream<27, false, false, S, R>;
-}
+// instantiation unit of one storage type and tile height (lbf_inst_<storage>_t<rows>.cu)
+#define LBF_INSTANTIATE(NAME, S, R, TYV)                                                                  \
+    StepLauncher step_launcher_##NAME##_t##TYV(int lat, int ho, int tc) { return step_table<S, R, TYV>(lat, ho, tc); } \
+    BatchOps batch_ops_##NAME##_t##TYV(int lat, int ho, int tc) { return batch_table<S, R, TYV>(lat, ho, tc); }
 
 }  // namespace lbf

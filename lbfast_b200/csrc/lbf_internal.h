@@ -28,27 +28,24 @@ struct StepArgs {
 
 using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
 
-// one table per storage type, defined in lbf_inst_<storage>.cu
-StepLauncher step_launcher_f32(int lat, int ho, int tc);
-StepLauncher step_launcher_f16(int lat, int ho, int tc);
-StepLauncher step_launcher_bf16(int lat, int ho, int tc);
-StepLauncher step_launcher_f64(int lat, int ho, int tc);
+// Step launcher of one kernel class (lattice 19/27, HIGHORDER, TWOCOMPONENT)
+// for a storage type and tile height (8 or 16 rows); nullptr if not built.
+StepLauncher step_launcher(int storage, int lat, int ho, int tc, int tile_y);
+bool tile_available(int storage, int tile_y);
 
-// Batched step of many boxes of one kernel class (lattice, HIGHORDER,
-// TWOCOMPONENT, storage): fill writes the device-format parameters of one box
-// (params_bytes bytes) from its StepArgs; launch runs one CTA per work item
-// (int4: box, tile x, tile y, z segment).
+// Batched step of many boxes of one kernel class and tile height: fill writes
+// the device-format parameters of one box (params_bytes bytes) from its
+// StepArgs; launch runs one CTA per work item (int4: box, tile x, tile y,
+// z segment).
 struct BatchOps {
     size_t params_bytes;
+    int tile_y;
     void (*fill)(const StepArgs&, void*);
     cudaError_t (*launch)(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st);
 };
-BatchOps batch_ops_f32(int lat, int ho, int tc);
-BatchOps batch_ops_f16(int lat, int ho, int tc);
-BatchOps batch_ops_bf16(int lat, int ho, int tc);
-BatchOps batch_ops_f64(int lat, int ho, int tc);
-// CTA tile of the step kernel (x, y) in nodes
-constexpr int STEP_TILE_X = 32, STEP_TILE_Y = 8;
+BatchOps batch_ops(int storage, int lat, int ho, int tc, int tile_y);
+// CTA tile width of the step kernel in nodes (the height is 8 or 16)
+constexpr int STEP_TILE_X = 32;
 
 // wetting tables (solid nodes whose ghost phi the reference updates)
 struct WetArgs {

@@ -80,12 +80,13 @@ struct Solve {
 };
 
 struct ClassKey {
-    int lat, ho, tc, storage;
+    int lat, ho, tc, storage, tile;
     bool operator<(const ClassKey& o) const {
         if (lat != o.lat) return lat < o.lat;
         if (ho != o.ho) return ho < o.ho;
         if (tc != o.tc) return tc < o.tc;
-        return storage < o.storage;
+        if (storage != o.storage) return storage < o.storage;
+        return tile < o.tile;
     }
 };
 
@@ -102,14 +103,8 @@ struct Batch {
     std::vector<int4> h_work;
 };
 
-lbf::BatchOps batch_ops(int storage, int lat, int ho, int tc) {
-    switch (storage) {
-        case LBF_STORE_F32: return lbf::batch_ops_f32(lat, ho, tc);
-        case LBF_STORE_F16: return lbf::batch_ops_f16(lat, ho, tc);
-        case LBF_STORE_BF16: return lbf::batch_ops_bf16(lat, ho, tc);
-        default: return lbf::batch_ops_f64(lat, ho, tc);
-    }
-}
+// tile height of a solve's class: the one requested, else 8 rows
+int solve_tile(const lbf_params& p) { return p.tile_y ? p.tile_y : 8; }
 
 // CTAs a batch should offer: three waves of two CTAs per SM on 148 SMs
 constexpr long long kTargetCtas = 148LL * 2 * 3;
@@ -200,10 +195,10 @@ int rebuild(lbf_server* s) {
     drop_graph(s);
     for (auto& kv : s->batches) kv.second.members.clear();
     for (Solve* v : s->active) {
-        ClassKey k{v->p.lattice, v->p.highorder, v->p.twocomponent, v->p.storage};
+        ClassKey k{v->p.lattice, v->p.highorder, v->p.twocomponent, v->p.storage, solve_tile(v->p)};
         Batch& b = s->batches[k];
         if (!b.ops.launch) {
-            b.ops = batch_ops(k.storage, k.lat, k.ho, k.tc);
+            b.ops = lbf::batch_ops(k.storage, k.lat, k.ho, k.tc, k.tile);
             if (!b.ops.launch) return sfail(LBF_E_UNSUPPORTED, "no batched kernel for this class");
             // sets the kernel's shared-memory attribute outside any graph capture
             SRV_TRY(b.ops.launch(nullptr, nullptr, 0, s->stream));
@@ -221,7 +216,7 @@ int rebuild(lbf_server* s) {
     long long cols = 0;
     for (Solve* v : s->active)
         cols += (long long)((v->p.lx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X) *
-                ((v->p.ly + lbf::STEP_TILE_Y - 1) / lbf::STEP_TILE_Y);
+                ((v->p.ly + solve_tile(v->p) - 1) / solve_tile(v->p));
     // z segments: as few as give the whole batch kTargetCtas CTAs (every
     // segment re-reads a few halo planes), at least 8 planes each
     const long long nseg = std::max<long long>(1, (kTargetCtas + cols - 1) / std::max<long long>(cols, 1));
@@ -245,7 +240,7 @@ int rebuild(lbf_server* s) {
             lbf::handle_step_args(&flipped, a, h->dr);
             b.ops.fill(a, b.h_params[1].data() + i * pb);
             const int gx = (h->nx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X;
-            const int gy = (h->ny + lbf::STEP_TILE_Y - 1) / lbf::STEP_TILE_Y;
+            const int gy = (h->ny + b.ops.tile_y - 1) / b.ops.tile_y;
             const int gz = (h->nz + h->zseg - 1) / h->zseg;
             for (int z = 0; z < gz; ++z)
                 for (int y = 0; y < gy; ++y)

@@ -10,7 +10,7 @@
 //   LB_int_boundary        (lb_cuda_boundary_module.f90:19-216)
 //   exchange_*_intpbc      (mpi_module.f90:2203-3286) -> periodic index wrap
 //
-// Work decomposition.  A CTA owns a TX x TY column of the box and sweeps a
+// Work decomposition.  A CTA owns a 32 x TY column of the box and sweeps a
 // segment of z planes.  For collision plane q it keeps in shared memory
 //   phi   planes q-1..q+3 on the tile + 3-node ring   (5-slot ring)
 //   theta = phi(1-phi) n on the tile + 2-node ring and g~ = n|grad phi| on
@@ -31,12 +31,20 @@
 
 namespace lbf {
 
-constexpr int TX = 32, TY = 8, NT = TX * TY;
-constexpr int R1X = TX + 2, R1Y = TY + 2, R1N = R1X * R1Y;  // collision region
-constexpr int R2X = TX + 4, R2Y = TY + 4, R2N = R2X * R2Y;  // theta region
-constexpr int R3X = TX + 6, R3Y = TY + 6, R3N = R3X * R3Y;  // phi region
-constexpr int NRING1 = R1N - NT;                              // 84 ring nodes of R1
+constexpr int TX = 32;                                   // tile width: one warp per tile row
+constexpr int R1X = TX + 2, R2X = TX + 4, R3X = TX + 6;  // region widths
 constexpr int PHI_SLOTS = 5, TH_SLOTS4 = 4;
+
+// A tile of TY_ rows (8 or 16) and its regions: collision R1 = tile + 1-node
+// ring, theta R2 = tile + 2, phi R3 = tile + 3.
+template <int TY_> struct Tile {
+    static constexpr int TY = TY_, NT = TX * TY_;
+    static constexpr int R1Y = TY_ + 2, R1N = R1X * R1Y;
+    static constexpr int R2Y = TY_ + 4, R2N = R2X * R2Y;
+    static constexpr int R3Y = TY_ + 6, R3N = R3X * R3Y;
+    static constexpr int NRING1 = R1N - NT;  // ring nodes of R1 (84 for 8 rows, 100 for 16)
+    static_assert(R2N <= 2 * NT && R3N <= 3 * NT, "region loops assume at most 2 / 3 nodes per thread");
+};
 
 __device__ __forceinline__ int wrap_coord(int g, int n, int periodic, bool& ok) {
     if (g < 0) {

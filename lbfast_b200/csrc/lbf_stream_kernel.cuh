@@ -50,7 +50,8 @@ constexpr int NSTAGE = 13;
 // 32/64-bit storage is prefetched with cp.async; 16-bit storage is read at the point of use
 template <typename S> constexpr bool staged() { return sizeof(S) >= 4; }
 
-template <int LAT, bool TC, typename S, typename R> constexpr size_t stream_smem_bytes_v2() {
+template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes_v2() {
+    constexpr int R1N = Tile<TYV>::R1N, R2N = Tile<TYV>::R2N, R3N = Tile<TYV>::R3N;
     size_t b = sizeof(R) * size_t(LAT) * R1N;
     if (TC) b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(TH_SLOTS4) * (3 * R2N + 3 * R1N));
     if (staged<S>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
@@ -58,8 +59,11 @@ template <int LAT, bool TC, typename S, typename R> constexpr size_t stream_smem
 }
 
 // One CTA's share of a time step: tile (bx, by) of the box, z segment bz.
-template <int LAT, bool HO, bool TC, typename S, typename R>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int bz) {
+    using TL = Tile<TYV>;
+    constexpr int TY = TL::TY, NT = TL::NT, NRING1 = TL::NRING1;
+    constexpr int R1Y = TL::R1Y, R1N = TL::R1N, R2Y = TL::R2Y, R2N = TL::R2N, R3N = TL::R3N;
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
     using CP = Codec<SP>;
@@ -625,24 +629,27 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     }
 }
 
+// CTAs per SM the kernel is compiled for: two of 256 threads, one of 512, one in FP64
+template <typename R, int TYV> constexpr int step_min_blocks() { return (sizeof(R) == 8 || TYV > 8) ? 1 : 2; }
+
 // Single box: one CTA per (tile x, tile y, z segment).
-template <int LAT, bool HO, bool TC, typename S, typename R>
-__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2)) stream_kernel(const StepParams<S, R> p) {
-    step_body<LAT, HO, TC, S, R>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+__global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
+    step_body<LAT, HO, TC, S, R, TYV>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many boxes in one launch: CTA i advances box work[i].x, tile (work[i].y,
 // work[i].z), z segment work[i].w, with that box's own parameters and fields.
 // Each node's arithmetic is the same as in stream_kernel, so a box gives the
 // same bits alone and in a batch.
-template <int LAT, bool HO, bool TC, typename S, typename R>
-__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 1 : 2))
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+__global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     stream_kernel_batched(const StepParams<S, R>* __restrict__ boxes, const int4* __restrict__ work) {
     __shared__ StepParams<S, R> sp;
     const int4 w = work[blockIdx.x];
     if (threadIdx.x == 0) sp = boxes[w.x];
     __syncthreads();
-    step_body<LAT, HO, TC, S, R>(sp, w.y, w.z, w.w);
+    step_body<LAT, HO, TC, S, R, TYV>(sp, w.y, w.z, w.w);
 }
 
 }  // namespace lbf

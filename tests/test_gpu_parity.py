@@ -101,3 +101,33 @@ def test_split_calls_equal_one_call():
     assert np.array_equal(ma, mb) and np.array_equal(pa, pb, equal_nan=True) and np.array_equal(ua, ub)
     a.close()
     b.close()
+
+
+def _fields_with(name, storage, nsteps, **over):
+    p, isf, m, phi = make_case(name, storage)
+    for k, v in over.items():
+        setattr(p, k, v)
+    s = Solver(p)
+    if p.obstacles:
+        s.set_isfluid(isf)
+    s.set_fields(m, phi)
+    s.step(nsteps)
+    out = s.get_fields()
+    s.close()
+    return out
+
+
+def _equal(a, b):
+    return all(x is None and y is None or np.array_equal(x, y, equal_nan=True) for x, y in zip(a, b))
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_tile_and_segment_do_not_change_results(name, storage):
+    """Tiles of 8 and 16 rows, several z segmentations and the autotuned choice
+    give the same bits: each node's arithmetic does not depend on the work
+    decomposition."""
+    ref = _fields_with(name, storage, 9, tile_y=8, zseg=0)
+    for over in ({"tile_y": 16, "zseg": 0}, {"tile_y": 16, "zseg": 5}, {"tile_y": 8, "zseg": 3},
+                 {"tile_y": 0, "zseg": 0}):
+        assert _equal(_fields_with(name, storage, 9, **over), ref), over
