@@ -134,6 +134,7 @@ def run_ours(args, rank, local, world):
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     p, m, phi = workload(args.storage, args.box)
+    p.tile_y, p.zseg = args.tile, args.zseg
     N = p.lx * p.ly * p.lz
     s = lbf.Solver(p)
     s.set_stream(stream.cuda_stream)
@@ -351,6 +352,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--box", type=int, default=LBOX)
+    ap.add_argument("--tile", type=int, default=0, help="kernel tile rows (8 or 16); 0: autotuned")
+    ap.add_argument("--zseg", type=int, default=0, help="planes per z segment; 0: autotuned / automatic")
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-solves", type=int, default=40, help="solves of the serving measurement (0: skip)")

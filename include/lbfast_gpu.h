@@ -68,7 +68,9 @@ typedef struct lbf_params {
                                 applies it only with WETTABILITY and otherwise uses 90
                                 (lb_cuda_boundary_module.f90:264,275) */
     int printphi;            /* PRINTPHI: `rho` output holds phi */
-    int zseg;                /* planes per z segment of the kernel; 0 = automatic */
+    int zseg;                /* planes per z segment of the kernel (one CTA per tile and segment); 0 = a
+                                persistent schedule: one CTA per resident slot, each advancing an equal
+                                contiguous share of the box's columns x planes */
     int tile_y;              /* rows of the kernel's 32-wide tile: 8 or 16 (FP64: 8 only); 0 = autotuned
                                 together with zseg (when zseg = 0) at the first lbf_step: each candidate
                                 (tile, zseg) is timed on the box itself, the fastest is kept and remembered
@@ -118,7 +120,8 @@ int lbf_sync(lbf_handle* h);
 
 /* Number of steps done since lbf_set_fields. */
 int lbf_get_step(lbf_handle* h, long long* step);
-/* The kernel tile height and z segment in use (after the autotuner, if it ran). */
+/* The kernel tile height and z segment (0: persistent schedule) in use, after
+ * the autotuner if it ran. */
 int lbf_get_tuning(lbf_handle* h, int* tile_y, int* zseg);
 
 /* State a next step starts from: moments (10 x N), phi (N) and the velocity

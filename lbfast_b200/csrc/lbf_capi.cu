@@ -141,8 +141,13 @@ int autotune(lbf_handle* h) {
         if (h->p.zseg > 0) {
             zs.push_back(std::min(h->p.zseg, h->nz));
         } else {
+            // the persistent schedule (0), and fixed segments: about four waves,
+            // half and twice that, and whole columns.  Segments keep the CTAs
+            // that run together on neighbouring columns at the same planes, so
+            // halo re-reads hit in L2; the persistent schedule balances the SMs
+            // exactly but staggers neighbours in z.
             const int za = auto_zseg(h->nx, h->ny, h->nz, ty), lo = std::min(h->nz, 8);
-            for (int z : {za, std::max(lo, za / 2), std::min(h->nz, 2 * za), h->nz})
+            for (int z : {0, za, std::max(lo, za / 2), std::min(h->nz, 2 * za), h->nz})
                 if (std::find(zs.begin(), zs.end(), z) == zs.end()) zs.push_back(z);
         }
         for (int z : zs) cand.emplace_back(ty, z);
@@ -324,7 +329,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
     }
-    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : auto_zseg(h->nx, h->ny, h->nz, h->tile_y);
+    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : 0;  // 0: persistent schedule
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
         ok = ok && cudaMalloc(&h->mom[b], 10 * h->N * h->esz) == cudaSuccess;

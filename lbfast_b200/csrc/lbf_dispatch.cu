@@ -2,6 +2,8 @@
 #include "../../include/lbfast_gpu.h"
 #include "lbf_internal.h"
 
+#include <algorithm>
+
 namespace lbf {
 
 StepLauncher step_launcher_f32_t8(int, int, int);
@@ -18,6 +20,23 @@ BatchOps batch_ops_f16_t16(int, int, int);
 BatchOps batch_ops_bf16_t8(int, int, int);
 BatchOps batch_ops_bf16_t16(int, int, int);
 BatchOps batch_ops_f64_t8(int, int, int);
+
+int resident_slots(int resident_per_sm) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 148;
+    }
+    return nsm * resident_per_sm;
+}
+
+// every resident CTA slot of the GPU, but no share shorter than 8 planes
+int persistent_grid(long long W, int resident_per_sm) {
+    constexpr long long MIN_SHARE = 8;
+    const long long slots = resident_slots(resident_per_sm);
+    return (int)std::max<long long>(1, std::min(slots, (W + MIN_SHARE - 1) / MIN_SHARE));
+}
 
 bool tile_available(int storage, int tile_y) {
     if (tile_y == 8) return true;

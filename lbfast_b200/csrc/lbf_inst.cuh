@@ -5,6 +5,8 @@
 #include "lbf_internal.h"
 #include "lbf_stream_kernel.cuh"
 
+#include <algorithm>
+
 namespace lbf {
 
 static_assert(TX == STEP_TILE_X, "host tile width must match the kernel's");
@@ -49,7 +51,20 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     }
     StepParams<S, R> p;
     make_params(a, p);
-    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
+    if (a.zseg > 0) {
+        dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
+        stream_kernel<LAT, HO, TC, S, R, TYV><<<grid, TX * TYV, smem, st>>>(p);
+        return cudaGetLastError();
+    }
+    static int resident = 0;  // CTAs per SM at this shared-memory size
+    if (!resident) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel<LAT, HO, TC, S, R, TYV>,
+                                                                      TX * TYV, smem);
+        if (e != cudaSuccess) return e;
+        if (resident < 1) return cudaErrorInvalidConfiguration;
+    }
+    const long long W = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV) * a.nz;
+    const int grid = persistent_grid(W, resident);
     stream_kernel<LAT, HO, TC, S, R, TYV><<<grid, TX * TYV, smem, st>>>(p);
     return cudaGetLastError();
 }
@@ -72,6 +87,20 @@ cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int n
     return cudaGetLastError();
 }
 
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV> int batched_resident() {
+    static int resident = 0;
+    if (!resident) {
+        const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
+        if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
+                                                          TX * TYV, smem) != cudaSuccess)
+            resident = 1;
+        resident = std::max(resident, 1);
+    }
+    return resident;
+}
+
 template <typename S, typename R> void fill_params(const StepArgs& a, void* dst) {
     make_params(a, *static_cast<StepParams<S, R>*>(dst));
 }
@@ -90,9 +119,19 @@ template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho,
     o.fill = &fill_params<S, R>;
     o.tile_y = TYV;
     o.launch = nullptr;
-    if (lat == 19 && !ho) o.launch = tc ? &launch_stream_batched<19, false, true, S, R, TYV> : &launch_stream_batched<19, false, false, S, R, TYV>;
-    if (lat == 27 && ho) o.launch = tc ? &launch_stream_batched<27, true, true, S, R, TYV> : &launch_stream_batched<27, true, false, S, R, TYV>;
-    if (lat == 27 && !ho) o.launch = tc ? &launch_stream_batched<27, false, true, S, R, TYV> : &launch_stream_batched<27, false, false, S, R, TYV>;
+    o.resident = nullptr;
+    if (lat == 19 && !ho) {
+        o.launch = tc ? &launch_stream_batched<19, false, true, S, R, TYV> : &launch_stream_batched<19, false, false, S, R, TYV>;
+        o.resident = tc ? &batched_resident<19, false, true, S, R, TYV> : &batched_resident<19, false, false, S, R, TYV>;
+    }
+    if (lat == 27 && ho) {
+        o.launch = tc ? &launch_stream_batched<27, true, true, S, R, TYV> : &launch_stream_batched<27, true, false, S, R, TYV>;
+        o.resident = tc ? &batched_resident<27, true, true, S, R, TYV> : &batched_resident<27, true, false, S, R, TYV>;
+    }
+    if (lat == 27 && !ho) {
+        o.launch = tc ? &launch_stream_batched<27, false, true, S, R, TYV> : &launch_stream_batched<27, false, false, S, R, TYV>;
+        o.resident = tc ? &batched_resident<27, false, true, S, R, TYV> : &batched_resident<27, false, false, S, R, TYV>;
+    }
     return o;
 }
 

@@ -35,14 +35,20 @@ bool tile_available(int storage, int tile_y);
 
 // Batched step of many boxes of one kernel class and tile height: fill writes
 // the device-format parameters of one box (params_bytes bytes) from its
-// StepArgs; launch runs one CTA per work item (int4: box, tile x, tile y,
-// z segment).
+// StepArgs; launch runs one CTA per work item (int4: box, first and end
+// column-plane of the box, column index = tile y * tiles in x + tile x, plane
+// fastest); resident gives the CTAs of the batched kernel one SM holds.
 struct BatchOps {
     size_t params_bytes;
     int tile_y;
     void (*fill)(const StepArgs&, void*);
     cudaError_t (*launch)(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st);
+    int (*resident)();
 };
+// resident CTA slots of the current GPU (SMs x CTAs per SM), and the CTAs of a
+// persistent launch over W column-planes (no share shorter than 8 planes)
+int resident_slots(int resident_per_sm);
+int persistent_grid(long long W, int resident_per_sm);
 BatchOps batch_ops(int storage, int lat, int ho, int tc, int tile_y);
 // CTA tile width of the step kernel in nodes (the height is 8 or 16)
 constexpr int STEP_TILE_X = 32;

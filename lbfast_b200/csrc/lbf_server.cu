@@ -106,9 +106,6 @@ struct Batch {
 // tile height of a solve's class: the one requested, else 8 rows
 int solve_tile(const lbf_params& p) { return p.tile_y ? p.tile_y : 8; }
 
-// CTAs a batch should offer: three waves of two CTAs per SM on 148 SMs
-constexpr long long kTargetCtas = 148LL * 2 * 3;
-
 }  // namespace
 
 struct lbf_server {
@@ -213,13 +210,6 @@ int rebuild(lbf_server* s) {
             ++it;
         }
     }
-    long long cols = 0;
-    for (Solve* v : s->active)
-        cols += (long long)((v->p.lx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X) *
-                ((v->p.ly + solve_tile(v->p) - 1) / solve_tile(v->p));
-    // z segments: as few as give the whole batch kTargetCtas CTAs (every
-    // segment re-reads a few halo planes), at least 8 planes each
-    const long long nseg = std::max<long long>(1, (kTargetCtas + cols - 1) / std::max<long long>(cols, 1));
     for (auto& kv : s->batches) {
         Batch& b = kv.second;
         std::stable_sort(b.members.begin(), b.members.end(), [](const Solve* a, const Solve* c) { return a->N > c->N; });
@@ -230,8 +220,6 @@ int rebuild(lbf_server* s) {
         b.h_work.clear();
         for (size_t i = 0; i < n; ++i) {
             lbf_handle* h = b.members[i]->h;
-            int zseg = (int)((h->nz + nseg - 1) / nseg);
-            h->zseg = std::max(zseg, std::min(h->nz, 8));
             lbf::StepArgs a;
             lbf::handle_step_args(h, a, h->dr);
             b.ops.fill(a, b.h_params[0].data() + i * pb);
@@ -239,12 +227,29 @@ int rebuild(lbf_server* s) {
             flipped.cur = 1 - h->cur;
             lbf::handle_step_args(&flipped, a, h->dr);
             b.ops.fill(a, b.h_params[1].data() + i * pb);
-            const int gx = (h->nx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X;
-            const int gy = (h->ny + b.ops.tile_y - 1) / b.ops.tile_y;
-            const int gz = (h->nz + h->zseg - 1) / h->zseg;
-            for (int z = 0; z < gz; ++z)
-                for (int y = 0; y < gy; ++y)
-                    for (int x = 0; x < gx; ++x) b.h_work.push_back(make_int4((int)i, x, y, z));
+        }
+        // z segments per column: whole columns when the batch has at least one
+        // wave of columns, else as many segments as still fit in one wave
+        // (every segment start recomputes a few planes); one work item per
+        // (member, segment, column), the columns of a segment consecutive so
+        // that neighbouring columns run at the same planes and their halo
+        // re-reads hit in L2
+        long long cols = 0;
+        for (Solve* v : b.members)
+            cols += (long long)((v->p.lx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X) *
+                    ((v->p.ly + b.ops.tile_y - 1) / b.ops.tile_y);
+        const long long slots = lbf::resident_slots(b.ops.resident());
+        const long long nseg = std::max<long long>(1, slots / std::max<long long>(cols, 1));
+        for (size_t i = 0; i < n; ++i) {
+            lbf_handle* h = b.members[i]->h;
+            const int ncol = ((h->nx + lbf::STEP_TILE_X - 1) / lbf::STEP_TILE_X) *
+                             ((h->ny + b.ops.tile_y - 1) / b.ops.tile_y);
+            const int zseg = std::max((int)((h->nz + nseg - 1) / nseg), std::min(h->nz, 8));
+            for (int z0 = 0; z0 < h->nz; z0 += zseg)
+                for (int c = 0; c < ncol; ++c) {
+                    const long long s0 = (long long)c * h->nz + z0;
+                    b.h_work.push_back(make_int4((int)i, (int)s0, (int)(s0 + std::min(zseg, h->nz - z0)), 0));
+                }
         }
         b.nwork = (int)b.h_work.size();
         if (b.params_cap < n * pb) {

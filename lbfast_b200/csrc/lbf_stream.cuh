@@ -13,8 +13,10 @@
 // Work decomposition.  A CTA owns a 32 x TY column of the box and sweeps a
 // segment of z planes.  For collision plane q it keeps in shared memory
 //   phi   planes q-1..q+3 on the tile + 3-node ring   (5-slot ring)
+//   in-plane partials of the separable phase-field stencils of phi (tile +
+//           2-node ring) and of theta (tile + 1-node ring)
 //   theta = phi(1-phi) n on the tile + 2-node ring and g~ = n|grad phi| on
-//           the tile + 1-node ring, planes q-1..q+2   (4-slot ring)
+//           the tile + 1-node ring
 //   the moments (and u_old) of plane q staged by cp.async
 //   post-collision populations of plane q on the tile + 1-node ring.
 // Each output node then pulls f*_l(x - c_l) from shared memory: the nine
@@ -33,7 +35,7 @@ namespace lbf {
 
 constexpr int TX = 32;                                   // tile width: one warp per tile row
 constexpr int R1X = TX + 2, R2X = TX + 4, R3X = TX + 6;  // region widths
-constexpr int PHI_SLOTS = 5, TH_SLOTS4 = 4;
+constexpr int PHI_SLOTS = 5;
 
 // A tile of TY_ rows (8 or 16) and its regions: collision R1 = tile + 1-node
 // ring, theta R2 = tile + 2, phi R3 = tile + 3.
@@ -56,7 +58,8 @@ __device__ __forceinline__ int wrap_coord(int g, int n, int periodic, bool& ok) 
 }
 
 // D3Q27 isotropic gradient of the reference (lb_cuda_auxfields_module.f90:72-100),
-// always with D3Q27 weights.  a(i,j,k) reads phi at offset (i,j,k).
+// always with D3Q27 weights (used by the wetting kernel; the step kernel
+// evaluates the same stencil in separable form).  a(i,j,k) reads phi at offset (i,j,k).
 template <typename R, typename A> __device__ __forceinline__ void iso_grad(const A& a, R& gx, R& gy, R& gz) {
     const R p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
     gx = R(3) * (p1 * (a(1, 0, 0) - a(-1, 0, 0)) +
@@ -74,39 +77,6 @@ template <typename R, typename A> __device__ __forceinline__ void iso_grad(const
                        (a(0, 1, 1) - a(0, -1, -1)) + (a(0, -1, 1) - a(0, 1, -1))) +
                  p3 * ((a(1, 1, 1) - a(-1, -1, -1)) + (a(-1, -1, 1) - a(1, 1, -1)) +
                        (a(1, -1, 1) - a(-1, 1, -1)) + (a(-1, 1, 1) - a(1, -1, -1))));
-}
-
-// isotropic Laplacian (lb_cuda_auxfields_module.f90:121-135)
-template <typename R, typename A> __device__ __forceinline__ R iso_lap(const A& a) {
-    const R p0 = R(8.0 / 27.0), p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
-    return R(6) * (a(0, 0, 0) * (p0 - R(1)) +
-                   (p1 * (a(1, 0, 0) + a(-1, 0, 0) + a(0, 1, 0) + a(0, -1, 0) + a(0, 0, 1) + a(0, 0, -1)) +
-                    p2 * ((a(1, 1, 0) + a(-1, -1, 0)) + (a(1, -1, 0) + a(-1, 1, 0)) + (a(1, 0, 1) + a(-1, 0, -1)) +
-                          (a(1, 0, -1) + a(-1, 0, 1)) + (a(0, 1, 1) + a(0, -1, -1)) + (a(0, 1, -1) + a(0, -1, 1))) +
-                    p3 * ((a(1, 1, 1) + a(-1, -1, -1)) + (a(1, -1, -1) + a(-1, 1, 1)) + (a(1, -1, 1) + a(-1, 1, -1)) +
-                          (a(1, 1, -1) + a(-1, -1, 1)))));
-}
-
-// divergence of theta (lb_cuda_auxfields_module.f90:1136-1157)
-template <typename R, typename AX, typename AY, typename AZ>
-__device__ __forceinline__ R iso_div(const AX& X, const AY& Y, const AZ& Z) {
-    const R p1 = R(2.0 / 27.0), p2 = R(1.0 / 54.0), p3 = R(1.0 / 216.0);
-    R dx = p1 * (X(1, 0, 0) - X(-1, 0, 0)) +
-           p2 * ((X(1, 1, 0) - X(-1, -1, 0)) + (X(1, -1, 0) - X(-1, 1, 0)) + (X(1, 0, 1) - X(-1, 0, -1)) +
-                 (X(1, 0, -1) - X(-1, 0, 1))) +
-           p3 * ((X(1, 1, 1) - X(-1, -1, -1)) + (X(1, -1, -1) - X(-1, 1, 1)) + (X(1, -1, 1) - X(-1, 1, -1)) +
-                 (X(1, 1, -1) - X(-1, -1, 1)));
-    R dy = p1 * (Y(0, 1, 0) - Y(0, -1, 0)) +
-           p2 * ((Y(1, 1, 0) - Y(-1, -1, 0)) + (Y(-1, 1, 0) - Y(1, -1, 0)) + (Y(0, 1, 1) - Y(0, -1, -1)) +
-                 (Y(0, 1, -1) - Y(0, -1, 1))) +
-           p3 * ((Y(1, 1, 1) - Y(-1, -1, -1)) + (Y(-1, 1, -1) - Y(1, -1, 1)) + (Y(1, 1, -1) - Y(-1, -1, 1)) +
-                 (Y(-1, 1, 1) - Y(1, -1, -1)));
-    R dz = p1 * (Z(0, 0, 1) - Z(0, 0, -1)) +
-           p2 * ((Z(1, 0, 1) - Z(-1, 0, -1)) + (Z(-1, 0, 1) - Z(1, 0, -1)) + (Z(0, 1, 1) - Z(0, -1, -1)) +
-                 (Z(0, -1, 1) - Z(0, 1, -1))) +
-           p3 * ((Z(1, 1, 1) - Z(-1, -1, -1)) + (Z(-1, -1, 1) - Z(1, 1, -1)) + (Z(1, -1, 1) - Z(-1, 1, -1)) +
-                 (Z(-1, 1, 1) - Z(1, -1, -1)));
-    return (dx + dy + dz) * R(3);
 }
 
 // 1-D D1Q3 inverse transform: Hermite coefficients (m0, m1, m2) -> values at c = -1, 0, +1

@@ -15,9 +15,15 @@
 
 namespace lbf {
 
+// Reciprocal and square root: in FP32 the hardware approximations (about 2 ulp)
+// instead of the correctly rounded sequences, which cost several instructions
+// and a branch each; FP64 stays correctly rounded.
 template <typename R> __device__ __forceinline__ R rcp(R x);
-template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ float rcp<float>(float x) { return __fdividef(1.0f, x); }
 template <> __device__ __forceinline__ double rcp<double>(double x) { return 1.0 / x; }
+template <typename R> __device__ __forceinline__ R sqrt_a(R x);
+template <> __device__ __forceinline__ float sqrt_a<float>(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+template <> __device__ __forceinline__ double sqrt_a<double>(double x) { return sqrt(x); }
 
 template <typename R>
 __device__ __forceinline__ void accum_slice(R (&acc)[10], R cz, R Y00, R Y01, R Y02, R Y10, R Y11, R Y20) {
@@ -47,20 +53,27 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // fields staged per collision node: 10 moments (+3 u_old with a density ratio)
 constexpr int NSTAGE = 13;
 
-// 32/64-bit storage is prefetched with cp.async; 16-bit storage is read at the point of use
-template <typename S> constexpr bool staged() { return sizeof(S) >= 4; }
+// FP32 storage is prefetched with cp.async; 16-bit and FP64 storage are read at
+// the point of use (FP64 leaves no shared memory for a staging area)
+template <typename S> constexpr bool staged() { return sizeof(S) == 4; }
+
+// ring slots of the separable phase-field stencils (see step_body)
+constexpr int SXY_SLOTS = 5, GXY_SLOTS = 3, TH_SLOTS = 2, GT_SLOTS = 3, H_SLOTS = 3;
 
 template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes_v2() {
     constexpr int R1N = Tile<TYV>::R1N, R2N = Tile<TYV>::R2N, R3N = Tile<TYV>::R3N;
     size_t b = sizeof(R) * size_t(LAT) * R1N;
-    if (TC) b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(TH_SLOTS4) * (3 * R2N + 3 * R1N));
+    if (TC)
+        b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(SXY_SLOTS) * R2N + size_t(GXY_SLOTS) * 2 * R2N +
+                          size_t(TH_SLOTS) * 3 * R2N + size_t(GT_SLOTS) * 3 * R1N + size_t(H_SLOTS) * 3 * R1N);
     if (staged<S>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
     return b;
 }
 
-// One CTA's share of a time step: tile (bx, by) of the box, z segment bz.
+// One piece of a time step: tile (bx, by) of the box, planes z0 <= z < z1.
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
-__device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int bz) {
+__device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int z0,
+                                          const int z1) {
     using TL = Tile<TYV>;
     constexpr int TY = TL::TY, NT = TL::NT, NRING1 = TL::NRING1;
     constexpr int R1Y = TL::R1Y, R1N = TL::R1N, R2Y = TL::R2Y, R2N = TL::R2N, R3N = TL::R3N;
@@ -71,16 +84,20 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* pops = reinterpret_cast<R*>(smem_raw);          // [LAT][R1N]
     R* phis = pops + LAT * R1N;                        // [PHI_SLOTS][R3N]     (TC)
-    R* ths = phis + (TC ? PHI_SLOTS * R3N : 0);        // [TH_SLOTS4][3][R2N]  (TC) theta
-    R* gts = ths + (TC ? TH_SLOTS4 * 3 * R2N : 0);     // [TH_SLOTS4][3][R1N]  (TC) g~
-    S* stg = reinterpret_cast<S*>(gts + (TC ? TH_SLOTS4 * 3 * R1N : 0));  // [NSTAGE][R1N] (STG)
+    R* sxys = phis + (TC ? PHI_SLOTS * R3N : 0);       // [SXY_SLOTS][R2N]     (TC) S_x S_y phi
+    R* gxys = sxys + (TC ? SXY_SLOTS * R2N : 0);       // [GXY_SLOTS][2][R2N]  (TC) D_x S_y phi, S_x D_y phi
+    R* ths = gxys + (TC ? GXY_SLOTS * 2 * R2N : 0);    // [TH_SLOTS][3][R2N]   (TC) theta
+    R* gts = ths + (TC ? TH_SLOTS * 3 * R2N : 0);      // [GT_SLOTS][3][R1N]   (TC) g~
+    R* hs = gts + (TC ? GT_SLOTS * 3 * R1N : 0);       // [H_SLOTS][3][R1N]    (TC) theta partials
+    S* stg = reinterpret_cast<S*>(hs + (TC ? H_SLOTS * 3 * R1N : 0));  // [NSTAGE][R1N] (STG)
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
     const int X0 = bx * TX, Y0 = by * TY;
-    const int z0 = bz * p.zseg;
-    const int z1 = min(z0 + p.zseg, p.nz);
-    const long long N = p.N, plane = p.plane;
+    // node indices inside one field fit in 32 bits (boxes hold < 2^31 nodes);
+    // field bases (f * N) are 64-bit and uniform across the CTA
+    const long long N = p.N;
+    const int plane = (int)p.plane;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const bool dr = TC && p.densratio;
     const bool obs = p.obstacles != 0;
@@ -113,7 +130,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     const bool okB = r1_geom(nodeB, offB);
     const int ox = X0 + tx, oy = Y0 + ty;
     const bool out_ok = (ox < nx) && (oy < ny);
-    const long long out_off = (long long)oy * nx + ox;
+    const int out_off = oy * nx + ox;
 
     // neighbour x / y coordinates of the output node (bounce-back isfluid tests)
     int nbx[3], nby[3];
@@ -160,8 +177,14 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     }
 
     auto zwrap = [&](int q, bool& ok) { return wrap_coord(q, nz, p.pbz, ok); };
-    auto phi_slot = [&](int q) { return (q - z0 + 3 + 4 * PHI_SLOTS) % PHI_SLOTS; };
-    auto th_slot = [&](int q) { return (q - z0 + 2 + 4 * TH_SLOTS4) % TH_SLOTS4; };
+    auto phi_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)PHI_SLOTS); };
+    auto sxy_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)SXY_SLOTS); };
+    auto gxy_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)GXY_SLOTS); };
+    auto th_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)TH_SLOTS); };
+    auto gt_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)GT_SLOTS); };
+    auto h_slot = [&](int q) { return (int)((unsigned)(q - z0 + 3) % (unsigned)H_SLOTS); };
+    // D1Q3 weights: the D3Q27 weights of the isotropic stencils factor as W(cx) W(cy) W(cz)
+    const R W0 = R(2.0 / 3.0), W1 = R(1.0 / 6.0);
 
     // phi plane q into its ring slot (zero outside the box); asynchronous or direct
     auto load_phi_plane = [&](int q, bool async) {
@@ -173,7 +196,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             const int n = t + k * NT;
             if (n < R3N) {
                 const bool ok = zok && r3_ok[k];
-                const long long g = (long long)wz * plane + r3_off[k];
+                const int g = wz * plane + r3_off[k];
                 if (async && ok) {
                     cp_async<sizeof(SP)>(dst + n, p.pin + g);
                 } else {
@@ -188,13 +211,13 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             bool zok = true;
             const int wz = zwrap(q, zok);
             if (!zok) return;
-            const long long zo = (long long)wz * plane;
+            const int zo = wz * plane;
 #pragma unroll 1
             for (int k = 0; k < 2; ++k) {
                 const int node = k ? nodeB : nodeA;
                 const bool ok = k ? okB : okA;
                 if (node < 0 || !ok) continue;
-                const long long g = zo + (k ? offB : offA);
+                const int g = zo + (k ? offB : offA);
 #pragma unroll
                 for (int f = 0; f < 10; ++f) cp_async<sizeof(S)>(stg + f * R1N + node, p.min + f * N + g);
                 if (dr) {
@@ -204,52 +227,121 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             }
         }
     };
+    // Separable phase-field stencils.  The isotropic gradient, Laplacian and
+    // divergence of the reference (lb_cuda_auxfields_module.f90:72-135,
+    // 1136-1157) use the D3Q27 weights w = W(cx) W(cy) W(cz), W(0) = 2/3,
+    // W(+-1) = 1/6, so each is a product of 1-D operators: S = W-weighted sum,
+    // D = W(1) x central difference.  Per plane the theta region keeps the
+    // in-plane partials S_x S_y phi, D_x S_y phi, S_x D_y phi; the z operator
+    // then combines three planes of them at the same (x, y):
+    //   grad phi = 3 (S_z D_x S_y, S_z S_x D_y, D_z S_x S_y) phi
+    //   lap phi  = 6 (S_z S_x S_y phi - phi)
+    // and likewise div theta = 3 (S_z (D_x S_y th_x + S_x D_y th_y) + D_z S_x S_y th_z)
+    // from in-plane partials of theta on the collision region.  The same sums
+    // as the reference, in another order.  The in-plane smoothings are kept
+    // relative to the node's own value (S_x S_y f - f_c, from the differences
+    // f - f_c), and z differences are taken of those and of the centre values
+    // separately: a z difference of two smoothed planes of values near 1
+    // would lose the digits that a small gradient needs in FP32.
+
+    // in-plane partials of phi(q) on this thread's theta-region nodes
+    auto planar_plane = [&](int q) {
+        const R* f = phis + phi_slot(q) * R3N;
+        R* sx = sxys + sxy_slot(q) * R2N;
+        R* gg = gxys + gxy_slot(q) * (2 * R2N);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int n = t + k * NT;
+            if (n >= R2N) continue;
+            const int hx = n % R2X, hy = n / R2X;
+            const R* c = f + (hy + 1) * R3X + (hx + 1);
+            const R fc = c[0];
+            R sr[3], dr_[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const R a = c[(r - 1) * R3X - 1], b = c[(r - 1) * R3X], e = c[(r - 1) * R3X + 1];
+                sr[r] = W1 * ((a - fc) + (e - fc)) + W0 * (b - fc);
+                dr_[r] = e - a;
+            }
+            sx[n] = W1 * (sr[0] + sr[2]) + W0 * sr[1];  // S_x S_y phi - phi_c
+            gg[n] = W1 * (W1 * (dr_[0] + dr_[2]) + W0 * dr_[1]);
+            gg[R2N + n] = W1 * (sr[2] - sr[0]);
+        }
+    };
     // theta = phi(1-phi) n on the theta region and g~ = n |g| on the collision
     // region of plane q (compute_norm_interface, lb_cuda_auxfields_module.f90:72-119)
+    // from the partials of planes q-1..q+1
     auto theta_plane = [&](int q) {
         bool zok = true;
         const int wz = zwrap(q, zok);
         const R* f0 = phis + phi_slot(q - 1) * R3N;
         const R* f1 = phis + phi_slot(q) * R3N;
         const R* f2 = phis + phi_slot(q + 1) * R3N;
+        const R* s0 = sxys + sxy_slot(q - 1) * R2N;
+        const R* s2 = sxys + sxy_slot(q + 1) * R2N;
+        const R* g0 = gxys + gxy_slot(q - 1) * (2 * R2N);
+        const R* g1 = gxys + gxy_slot(q) * (2 * R2N);
+        const R* g2 = gxys + gxy_slot(q + 1) * (2 * R2N);
         R* th = ths + th_slot(q) * (3 * R2N);
-        R* gt = gts + th_slot(q) * (3 * R1N);
+        R* gt = gts + gt_slot(q) * (3 * R1N);
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const int n = t + k * NT;
             if (n >= R2N) continue;
             const int hx = n % R2X, hy = n / R2X;
-            const int c3 = (hy + 1) * R3X + (hx + 1);
             bool fluid = zok && r2_ok[k];
             if (fluid && obs) {
-                const int s = p.isf[(long long)wz * plane + r2_off[k]];
+                const int s = p.isf[wz * plane + r2_off[k]];
                 fluid = (s == 1 || s == -1);
             }
-            R th0 = 0, th1 = 0, th2 = 0, g0 = 0, g1 = 0, g2 = 0;
+            R th0 = 0, th1 = 0, th2 = 0, gv0 = 0, gv1 = 0, gv2 = 0;
             if (fluid) {
-                auto A = [&](int a, int b, int c) -> R {
-                    const R* f = c < 0 ? f0 : (c > 0 ? f2 : f1);
-                    return f[c3 + b * R3X + a];
-                };
-                R gx, gy, gz;
-                iso_grad<R>(A, gx, gy, gz);
-                const R mg = sqrt(gx * gx + gy * gy + gz * gz);
+                const R gx = R(3) * (W1 * (g0[n] + g2[n]) + W0 * g1[n]);
+                const R gy = R(3) * (W1 * (g0[R2N + n] + g2[R2N + n]) + W0 * g1[R2N + n]);
+                const int c3 = (hy + 1) * R3X + (hx + 1);
+                const R gz = R(3) * W1 * ((s2[n] - s0[n]) + (f2[c3] - f0[c3]));
+                const R mg = sqrt_a<R>(gx * gx + gy * gy + gz * gz);
                 const R rden = rcp<R>(mg + R(1.0e-9));
                 const R nxv = gx * rden, nyv = gy * rden, nzv = gz * rden;
                 const R ph = f1[c3];
                 const R pp = ph * (R(1) - ph);
                 th0 = pp * nxv; th1 = pp * nyv; th2 = pp * nzv;
-                g0 = nxv * mg; g1 = nyv * mg; g2 = nzv * mg;
+                gv0 = nxv * mg; gv1 = nyv * mg; gv2 = nzv * mg;
             }
             th[0 * R2N + n] = th0;
             th[1 * R2N + n] = th1;
             th[2 * R2N + n] = th2;
             if (hx >= 1 && hx <= R2X - 2 && hy >= 1 && hy <= R2Y - 2) {
                 const int n1 = (hy - 1) * R1X + (hx - 1);
-                gt[0 * R1N + n1] = g0;
-                gt[1 * R1N + n1] = g1;
-                gt[2 * R1N + n1] = g2;
+                gt[0 * R1N + n1] = gv0;
+                gt[1 * R1N + n1] = gv1;
+                gt[2 * R1N + n1] = gv2;
             }
+        }
+    };
+    // in-plane partials of theta(q) at this thread's collision nodes:
+    // D_x S_y th_x + S_x D_y th_y and S_x S_y th_z
+    auto theta_partials = [&](int q) {
+        const R* th = ths + th_slot(q) * (3 * R2N);
+        R* h = hs + h_slot(q) * (3 * R1N);
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            const int node = k ? nodeB : nodeA;
+            if (node < 0) continue;
+            const int hx = node % R1X, hy = node / R1X;
+            const R* c = th + (hy + 1) * R2X + (hx + 1);
+            const R zc = c[2 * R2N];
+            R dx[3], sy[3], sz[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int o = (r - 1) * R2X;
+                dx[r] = c[o + 1] - c[o - 1];
+                sy[r] = W1 * (c[R2N + o - 1] + c[R2N + o + 1]) + W0 * c[R2N + o];
+                sz[r] = W1 * ((c[2 * R2N + o - 1] - zc) + (c[2 * R2N + o + 1] - zc)) + W0 * (c[2 * R2N + o] - zc);
+            }
+            h[node] = W1 * (W1 * (dx[0] + dx[2]) + W0 * dx[1]) + W1 * (sy[2] - sy[0]);
+            h[R1N + node] = W1 * (sz[0] + sz[2]) + W0 * sz[1];  // S_x S_y th_z - th_z,c
+            h[2 * R1N + node] = zc;
         }
     };
 
@@ -261,12 +353,23 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 
     // ---- prologue: phi(z0-3..z0+2), theta(z0-2..z0), staged moments of plane z0-1 ----
     if constexpr (TC) {
+        // partials of phi(z0-3..z0+1), theta(z0-2..z0), theta partials (z0-2, z0-1)
+        // (theta reads only this thread's own partials; the partial slots are
+        // reused as soon as a theta plane no longer needs them)
         for (int q = z0 - 3; q <= z0 + 1; ++q) load_phi_plane(q, false);
         __syncthreads();
+        planar_plane(z0 - 3);
+        planar_plane(z0 - 2);
+        planar_plane(z0 - 1);
         theta_plane(z0 - 2);
+        planar_plane(z0);
         theta_plane(z0 - 1);
+        planar_plane(z0 + 1);
         __syncthreads();
-        theta_plane(z0);               // reads phi(z0-1..z0+1)
+        theta_partials(z0 - 2);
+        theta_partials(z0 - 1);
+        __syncthreads();
+        theta_plane(z0);               // into the slot of theta(z0-2)
         load_phi_plane(z0 + 2, true);  // into the slot of phi(z0-3), no longer read
     }
     stage_plane(z0 - 1);
@@ -276,19 +379,25 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     for (int q = z0 - 1; q <= z1; ++q) {
         bool zok = true;
         const int wz = zwrap(q, zok);
-        const long long zoff = (long long)wz * plane;
+        const int zoff = wz * plane;
         const bool q_inner = (q >= z0) && (q < z1);
 
         // ================= phase 1 =================
-        // theta(q+2) reads phi(q+1..q+3) and replaces theta(q-2)
-        if constexpr (TC) theta_plane(q + 2);
+        // partials of phi(q+3), then theta(q+2) from the partials of planes
+        // q+1..q+3 (this thread's own nodes), and the theta partials of plane
+        // q+1 at this thread's collision nodes
+        if constexpr (TC) {
+            planar_plane(q + 3);
+            theta_plane(q + 2);
+            theta_partials(q + 1);
+        }
 
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             const int node = k ? nodeB : nodeA;
             if (node < 0) continue;
             const bool inb = zok && (k ? okB : okA);
-            const long long gi = zoff + (k ? offB : offA);
+            const int gi = zoff + (k ? offB : offA);
             int isf = 1;
             if (inb && obs) isf = p.isf[gi];
             const bool live = inb && (isf != 0);
@@ -303,16 +412,17 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     pxx = (R)stg[4 * R1N + node]; pyy = (R)stg[5 * R1N + node]; pzz = (R)stg[6 * R1N + node];
                     pxy = (R)stg[7 * R1N + node]; pxz = (R)stg[8 * R1N + node]; pyz = (R)stg[9 * R1N + node];
                 } else {
-                    P = (R)__ldg(p.pres_in + gi);
-                    u = CD::ld(p.min, 1 * N + gi, p.inv_scale[1]);
-                    v = CD::ld(p.min, 2 * N + gi, p.inv_scale[2]);
-                    w = CD::ld(p.min, 3 * N + gi, p.inv_scale[3]);
-                    pxx = CD::ld(p.min, 4 * N + gi, p.inv_scale[4]);
-                    pyy = CD::ld(p.min, 5 * N + gi, p.inv_scale[5]);
-                    pzz = CD::ld(p.min, 6 * N + gi, p.inv_scale[6]);
-                    pxy = CD::ld(p.min, 7 * N + gi, p.inv_scale[7]);
-                    pxz = CD::ld(p.min, 8 * N + gi, p.inv_scale[8]);
-                    pyz = CD::ld(p.min, 9 * N + gi, p.inv_scale[9]);
+                    if constexpr (CD::scaled) P = (R)__ldg(p.pres_in + gi);
+                    else P = CD::ld(p.min + 0 * N, gi, p.inv_scale[0]);
+                    u = CD::ld(p.min + 1 * N, gi, p.inv_scale[1]);
+                    v = CD::ld(p.min + 2 * N, gi, p.inv_scale[2]);
+                    w = CD::ld(p.min + 3 * N, gi, p.inv_scale[3]);
+                    pxx = CD::ld(p.min + 4 * N, gi, p.inv_scale[4]);
+                    pyy = CD::ld(p.min + 5 * N, gi, p.inv_scale[5]);
+                    pzz = CD::ld(p.min + 6 * N, gi, p.inv_scale[6]);
+                    pxy = CD::ld(p.min + 7 * N, gi, p.inv_scale[7]);
+                    pxz = CD::ld(p.min + 8 * N, gi, p.inv_scale[8]);
+                    pyz = CD::ld(p.min + 9 * N, gi, p.inv_scale[9]);
                     if constexpr (CD::scaled) {
                         // 16-bit storage keeps Pi - u u, the deviation from equilibrium
                         pxx += u * u; pyy += v * v; pzz += w * w;
@@ -322,34 +432,21 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 R phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
                 if constexpr (TC) {
                     const int hx = node % R1X, hy = node / R1X;
-                    const int c3 = (hy + 2) * R3X + (hx + 2);
                     const int c2 = (hy + 1) * R2X + (hx + 1);
-                    const R* f0 = phis + phi_slot(q - 1) * R3N;
-                    const R* f1 = phis + phi_slot(q) * R3N;
-                    const R* f2 = phis + phi_slot(q + 1) * R3N;
-                    auto A = [&](int a, int b, int c) -> R {
-                        const R* f = c < 0 ? f0 : (c > 0 ? f2 : f1);
-                        return f[c3 + b * R3X + a];
-                    };
-                    phi = f1[c3];
-                    lap = iso_lap<R>(A);
-                    const R* t0 = ths + th_slot(q - 1) * (3 * R2N);
-                    const R* t1 = ths + th_slot(q) * (3 * R2N);
-                    const R* t2 = ths + th_slot(q + 1) * (3 * R2N);
-                    auto TXa = [&](int a, int b, int c) -> R {
-                        const R* f = c < 0 ? t0 : (c > 0 ? t2 : t1);
-                        return f[0 * R2N + c2 + b * R2X + a];
-                    };
-                    auto TYa = [&](int a, int b, int c) -> R {
-                        const R* f = c < 0 ? t0 : (c > 0 ? t2 : t1);
-                        return f[1 * R2N + c2 + b * R2X + a];
-                    };
-                    auto TZa = [&](int a, int b, int c) -> R {
-                        const R* f = c < 0 ? t0 : (c > 0 ? t2 : t1);
-                        return f[2 * R2N + c2 + b * R2X + a];
-                    };
-                    divt = iso_div<R>(TXa, TYa, TZa);
-                    const R* g1 = gts + th_slot(q) * (3 * R1N);
+                    const int c3 = (hy + 2) * R3X + (hx + 2);
+                    phi = phis[phi_slot(q) * R3N + c3];
+                    const R phm = phis[phi_slot(q - 1) * R3N + c3], php = phis[phi_slot(q + 1) * R3N + c3];
+                    const R* sm = sxys + sxy_slot(q - 1) * R2N;
+                    const R* s0 = sxys + sxy_slot(q) * R2N;
+                    const R* sp = sxys + sxy_slot(q + 1) * R2N;
+                    // S_z S_x S_y phi - phi, with W0 - 1 = -2 W1
+                    lap = R(6) * (W1 * (sm[c2] + sp[c2]) + W0 * s0[c2] + W1 * ((phm - phi) + (php - phi)));
+                    const R* hm = hs + h_slot(q - 1) * (3 * R1N);
+                    const R* h0 = hs + h_slot(q) * (3 * R1N);
+                    const R* hp = hs + h_slot(q + 1) * (3 * R1N);
+                    divt = R(3) * ((W1 * (hm[node] + hp[node]) + W0 * h0[node]) +
+                                   W1 * ((hp[R1N + node] - hm[R1N + node]) + (hp[2 * R1N + node] - hm[2 * R1N + node])));
+                    const R* g1 = gts + gt_slot(q) * (3 * R1N);
                     gfx = g1[0 * R1N + node];
                     gfy = g1[1 * R1N + node];
                     gfz = g1[2 * R1N + node];
@@ -383,9 +480,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     if constexpr (STG) {
                         uo = (R)stg[10 * R1N + node]; vo = (R)stg[11 * R1N + node]; wo = (R)stg[12 * R1N + node];
                     } else {
-                        uo = CD::ld(p.uin, 0 * N + gi, p.inv_scale[F_UOLD + 0]);
-                        vo = CD::ld(p.uin, 1 * N + gi, p.inv_scale[F_UOLD + 1]);
-                        wo = CD::ld(p.uin, 2 * N + gi, p.inv_scale[F_UOLD + 2]);
+                        uo = CD::ld(p.uin + 0 * N, gi, p.inv_scale[F_UOLD + 0]);
+                        vo = CD::ld(p.uin + 1 * N, gi, p.inv_scale[F_UOLD + 1]);
+                        wo = CD::ld(p.uin + 2 * N, gi, p.inv_scale[F_UOLD + 2]);
                     }
                     const R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
                     const R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
@@ -432,9 +529,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 // ---- outputs of this node that leave the kernel ----
                 if (interior) {
                     if (p.write_u) {
-                        CD::st(p.uout, 0 * N + gi, u, p.scale[F_UOLD + 0]);
-                        CD::st(p.uout, 1 * N + gi, v, p.scale[F_UOLD + 1]);
-                        CD::st(p.uout, 2 * N + gi, w, p.scale[F_UOLD + 2]);
+                        CD::st(p.uout + 0 * N, gi, u, p.scale[F_UOLD + 0]);
+                        CD::st(p.uout + 1 * N, gi, v, p.scale[F_UOLD + 1]);
+                        CD::st(p.uout + 2 * N, gi, w, p.scale[F_UOLD + 2]);
                     }
                     if constexpr (TC) {
                         // update_phifields: lb_cuda_update_phi_module.f90:77-93
@@ -545,7 +642,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     bool zk = true;
                     const int zz = zwrap(q - cz, zk);
                     int s = 1;
-                    if (nbx_ok[ix] && nby_ok[iy] && zk) s = p.isf[(long long)zz * plane + (long long)nby[iy] * nx + nbx[ix]];
+                    if (nbx_ok[ix] && nby_ok[iy] && zk) s = p.isf[zz * plane + nby[iy] * nx + nbx[ix]];
                     if (s != 0) continue;
                     const R wl = R(WL<LAT>(l));
                     const R dx = R(cx), dy = R(cy), dz = R(cz);
@@ -600,23 +697,23 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             else accum_slice<R>(ap, R(cz), Y00, Y01, Y02, Y10, Y11, Y20);
         }
         if (q - 1 >= z0 && out_ok) {
-            const long long go = (long long)(q - 1) * plane + out_off;
+            const int go = (q - 1) * plane + out_off;
             const R third = am[0] * cssq;
             if constexpr (CD::scaled) {
                 am[4] -= am[1] * am[1]; am[5] -= am[2] * am[2]; am[6] -= am[3] * am[3];
                 am[7] -= am[1] * am[2]; am[8] -= am[1] * am[3]; am[9] -= am[2] * am[3];
             }
             if constexpr (CD::scaled) p.pres_out[go] = (float)am[0];
-            else CD::st(p.mout, 0 * N + go, am[0], p.scale[0]);
-            CD::st(p.mout, 1 * N + go, am[1], p.scale[1]);
-            CD::st(p.mout, 2 * N + go, am[2], p.scale[2]);
-            CD::st(p.mout, 3 * N + go, am[3], p.scale[3]);
-            CD::st(p.mout, 4 * N + go, am[4] - third, p.scale[4]);
-            CD::st(p.mout, 5 * N + go, am[5] - third, p.scale[5]);
-            CD::st(p.mout, 6 * N + go, am[6] - third, p.scale[6]);
-            CD::st(p.mout, 7 * N + go, am[7], p.scale[7]);
-            CD::st(p.mout, 8 * N + go, am[8], p.scale[8]);
-            CD::st(p.mout, 9 * N + go, am[9], p.scale[9]);
+            else CD::st(p.mout + 0 * N, go, am[0], p.scale[0]);
+            CD::st(p.mout + 1 * N, go, am[1], p.scale[1]);
+            CD::st(p.mout + 2 * N, go, am[2], p.scale[2]);
+            CD::st(p.mout + 3 * N, go, am[3], p.scale[3]);
+            CD::st(p.mout + 4 * N, go, am[4] - third, p.scale[4]);
+            CD::st(p.mout + 5 * N, go, am[5] - third, p.scale[5]);
+            CD::st(p.mout + 6 * N, go, am[6] - third, p.scale[6]);
+            CD::st(p.mout + 7 * N, go, am[7], p.scale[7]);
+            CD::st(p.mout + 8 * N, go, am[8], p.scale[8]);
+            CD::st(p.mout + 9 * N, go, am[9], p.scale[9]);
         }
 #pragma unroll
         for (int i = 0; i < 10; ++i) {
@@ -632,16 +729,43 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 // CTAs per SM the kernel is compiled for: two of 256 threads, one of 512, one in FP64
 template <typename R, int TYV> constexpr int step_min_blocks() { return (sizeof(R) == 8 || TYV > 8) ? 1 : 2; }
 
-// Single box: one CTA per (tile x, tile y, z segment).
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
-__global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
-    step_body<LAT, HO, TC, S, R, TYV>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+// Column-planes of a box for a tile of TYV rows, column index = by * gx + bx.
+template <int TYV, typename F>
+__device__ __forceinline__ void run_share(const int nx, const int ny, const int nz, long long s0, long long s1,
+                                          F&& body) {
+    const int gx = (nx + TX - 1) / TX;
+    while (s0 < s1) {
+        const long long col = s0 / nz;
+        const int z0 = (int)(s0 - col * nz);
+        const int z1 = (int)min((long long)nz, z0 + (s1 - s0));
+        body((int)(col % gx), (int)(col / gx), z0, z1);
+        s0 += z1 - z0;
+    }
 }
 
-// Many boxes in one launch: CTA i advances box work[i].x, tile (work[i].y,
-// work[i].z), z segment work[i].w, with that box's own parameters and fields.
-// Each node's arithmetic is the same as in stream_kernel, so a box gives the
-// same bits alone and in a batch.
+// Single box.  zseg > 0: one CTA per (tile x, tile y, z segment of zseg
+// planes).  zseg = 0: persistent schedule -- the box's columns x planes are
+// cut into gridDim.x equal contiguous shares (a share may end inside one
+// column and continue at the bottom of the next), so every CTA does the same
+// work and pays the pipeline fill of a segment start only once or twice.
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+__global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
+    if (p.zseg > 0) {
+        const int z0 = blockIdx.z * p.zseg;
+        step_body<LAT, HO, TC, S, R, TYV>(p, blockIdx.x, blockIdx.y, z0, min(z0 + p.zseg, p.nz));
+        return;
+    }
+    const long long W = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV) * p.nz;
+    const long long share = (W + gridDim.x - 1) / gridDim.x;
+    const long long s0 = (long long)blockIdx.x * share;
+    run_share<TYV>(p.nx, p.ny, p.nz, s0, min(W, s0 + share),
+                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV>(p, bx, by, z0, z1); });
+}
+
+// Many boxes in one launch: CTA i advances box work[i].x over column-planes
+// [work[i].y, work[i].z) of that box (column-major: plane fastest), with the
+// box's own parameters and fields.  Each node's arithmetic is the same as in
+// stream_kernel, so a box gives the same bits alone and in a batch.
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     stream_kernel_batched(const StepParams<S, R>* __restrict__ boxes, const int4* __restrict__ work) {
@@ -649,7 +773,8 @@ __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     const int4 w = work[blockIdx.x];
     if (threadIdx.x == 0) sp = boxes[w.x];
     __syncthreads();
-    step_body<LAT, HO, TC, S, R, TYV>(sp, w.y, w.z, w.w);
+    run_share<TYV>(sp.nx, sp.ny, sp.nz, w.y, w.z,
+                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV>(sp, bx, by, z0, z1); });
 }
 
 }  // namespace lbf
