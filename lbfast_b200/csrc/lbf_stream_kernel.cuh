@@ -60,9 +60,14 @@ template <typename S> constexpr bool staged() { return sizeof(S) == 4; }
 // ring slots of the separable phase-field stencils (see step_body)
 constexpr int SXY_SLOTS = 5, GXY_SLOTS = 3, TH_SLOTS = 2, GT_SLOTS = 3, H_SLOTS = 3;
 
+// vector of two R (the populations of cz = -1 and 0 of one (cx, cy) group)
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
 template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes_v2() {
     constexpr int R1N = Tile<TYV>::R1N, R2N = Tile<TYV>::R2N, R3N = Tile<TYV>::R3N;
-    size_t b = sizeof(R) * size_t(LAT) * R1N;
+    size_t b = sizeof(R) * size_t(27) * R1N;  // populations: 9 (cx, cy) groups x 3 cz
     if (TC)
         b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(SXY_SLOTS) * R2N + size_t(GXY_SLOTS) * 2 * R2N +
                           size_t(TH_SLOTS) * 3 * R2N + size_t(GT_SLOTS) * 3 * R1N + size_t(H_SLOTS) * 3 * R1N);
@@ -82,8 +87,12 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     using CP = Codec<SP>;
     constexpr bool STG = staged<S>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* pops = reinterpret_cast<R*>(smem_raw);          // [LAT][R1N]
-    R* phis = pops + LAT * R1N;                        // [PHI_SLOTS][R3N]     (TC)
+    // post-collision populations of plane q, by (cx, cy) group g = 3 (cy+1) + (cx+1):
+    // the output nodes that read one group of a node read all three cz of it
+    using R2 = typename Vec2<R>::type;
+    R2* pops2 = reinterpret_cast<R2*>(smem_raw);                  // [9][R1N] (cz = -1, cz = 0)
+    R* pops1 = reinterpret_cast<R*>(pops2 + 9 * R1N);             // [9][R1N] (cz = +1)
+    R* phis = pops1 + 9 * R1N;                         // [PHI_SLOTS][R3N]     (TC)
     R* sxys = phis + (TC ? PHI_SLOTS * R3N : 0);       // [SXY_SLOTS][R2N]     (TC) S_x S_y phi
     R* gxys = sxys + (TC ? SXY_SLOTS * R2N : 0);       // [GXY_SLOTS][2][R2N]  (TC) D_x S_y phi, S_x D_y phi
     R* ths = gxys + (TC ? GXY_SLOTS * 2 * R2N : 0);    // [TH_SLOTS][3][R2N]   (TC) theta
@@ -630,7 +639,16 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 for (int l = 0; l < LAT; ++l) fpop[l] = R(0);
             }
 #pragma unroll
-            for (int l = 0; l < LAT; ++l) pops[l * R1N + node] = fpop[l];
+            for (int g = 0; g < 9; ++g) {
+                const int cx = g % 3 - 1, cy = g / 3 - 1;
+                constexpr bool q19 = LAT == 19;
+                const bool has_z = !q19 || (cx * cx + cy * cy) < 2;  // D3Q19 has no (+-1, +-1, +-1)
+                R2 v;
+                v.x = has_z ? fpop[LINK(cx, cy, -1)] : R(0);
+                v.y = fpop[LINK(cx, cy, 0)];
+                pops2[g * R1N + node] = v;
+                pops1[g * R1N + node] = has_z ? fpop[LINK(cx, cy, 1)] : R(0);
+            }
 
             // ---- obstacle bounce-back: lb_cuda_boundary_module.f90:162-199 ----
             if (interior && obs && isf == -1) {
@@ -664,24 +682,26 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         if (q < z1) stage_plane(q + 1);
         if constexpr (TC) load_phi_plane(q + 4, true);
 
+        // the three cz populations of every (cx, cy) group from node x - c
+        R gv[3][3][3];  // [cz][cy][cx]
+#pragma unroll
+        for (int yc = 0; yc < 3; ++yc)
+#pragma unroll
+            for (int xc = 0; xc < 3; ++xc) {
+                const int g = 3 * yc + xc;
+                const int src = (ty + 1 - (yc - 1)) * R1X + (tx + 1 - (xc - 1));
+                const R2 v = pops2[g * R1N + src];
+                gv[0][yc][xc] = v.x;
+                gv[1][yc][xc] = v.y;
+                gv[2][yc][xc] = pops1[g * R1N + src];
+            }
 #pragma unroll
         for (int zc = 0; zc < 3; ++zc) {
             const int cz = zc - 1;
             R S0[3], S1[3], S2[3];
 #pragma unroll
             for (int yc = 0; yc < 3; ++yc) {
-                const int cy = yc - 1;
-                R g[3];
-#pragma unroll
-                for (int xc = 0; xc < 3; ++xc) {
-                    const int cx = xc - 1;
-                    const int l = LINK(cx, cy, cz);
-                    if (LAT == 19 && (cx * cx + cy * cy + cz * cz) == 3) {
-                        g[xc] = R(0);
-                    } else {
-                        g[xc] = pops[l * R1N + (ty + 1 - cy) * R1X + (tx + 1 - cx)];
-                    }
-                }
+                const R* g = gv[zc][yc];
                 S0[yc] = g[0] + g[1] + g[2];
                 S1[yc] = g[2] - g[0];
                 S2[yc] = g[2] + g[0];
