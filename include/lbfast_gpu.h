@@ -75,6 +75,11 @@ typedef struct lbf_params {
                                 together with zseg (when zseg = 0) at the first lbf_step: each candidate
                                 (tile, zseg) is timed on the box itself, the fastest is kept and remembered
                                 for boxes of the same shape and class.  Results do not depend on either. */
+    int phi_correction;      /* two components: after every step restore the FP64 sum of phi over fluid
+                                nodes to its value at the first step by adding (sum0 - sum) / count to
+                                the count interface nodes with 0.5 < phi < 0.9 (the reference's
+                                BCPHIFLUX Lagrange correction, boundary_cds_module.f90:1864-1885, which it
+                                applies with open boundaries only); 0 = off (the reference default) */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;

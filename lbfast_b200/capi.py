@@ -40,7 +40,7 @@ class LbfParams(C.Structure):
         ("visc1", C.c_double), ("visc2", C.c_double), ("rho_r", C.c_double), ("rho_b", C.c_double),
         ("sigma", C.c_double), ("width", C.c_double), ("tau_diff", C.c_double),
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
-        ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int),
+        ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int), ("phi_correction", C.c_int),
     ]
 
 
@@ -155,6 +155,7 @@ class Params:
     printphi: int = 0
     zseg: int = 0
     tile_y: int = 0
+    phi_correction: int = 0
 
     def to_c(self) -> LbfParams:
         p = LbfParams()

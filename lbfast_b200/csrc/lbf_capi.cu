@@ -85,6 +85,7 @@ void free_all(lbf_handle* h) {
     cudaFree(h->wet_shift);
     cudaFree(h->d_err);
     cudaFree(h->d_red);
+    cudaFree(h->d_mass);
     cudaFree(h->staging);
 }
 
@@ -243,6 +244,9 @@ int flush_wet(lbf_handle* h) {
 }
 
 int prime(lbf_handle* h) {
+    if (h->d_mass)
+        CUDA_TRY(lbf::launch_mass(h->storage, true, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass,
+                                  h->stream));
     int rc = launch_wet(h, h->cur, 1 - h->cur, true);
     if (rc) return rc;
     h->primed = true;
@@ -288,6 +292,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (p->visc1 <= 0 || (p->twocomponent && p->visc2 <= 0)) return fail(LBF_E_ARG, "viscosities must be positive");
     if (p->twocomponent && (p->width <= 0)) return fail(LBF_E_ARG, "interface width must be positive");
     if (p->densratio && (p->rho_r <= 0 || p->rho_b <= 0)) return fail(LBF_E_ARG, "densities must be positive");
+    if (p->phi_correction && !p->twocomponent) return fail(LBF_E_ARG, "phi_correction requires TWOCOMPONENT");
     lbf_handle* h = new (std::nothrow) lbf_handle();
     if (!h) return fail(LBF_E_NOMEM, "host allocation failed");
     h->p = *p;
@@ -340,6 +345,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (ok && h->obs) ok = cudaMalloc(&h->isf, h->N) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_red, 5 * sizeof(double)) == cudaSuccess;
+    if (ok && p->phi_correction) ok = cudaMalloc(&h->d_mass, 3 * sizeof(double)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         free_all(h);
@@ -572,6 +578,8 @@ int lbf_step(lbf_handle* h, int nsteps) {
         cudaError_t e = h->launcher(a, h->stream);
         if (e != cudaSuccess) return fail(LBF_E_CUDA, "step kernel launch: %s", cudaGetErrorString(e));
         lbf::handle_advance(h, write_u);
+        rc = lbf::handle_post_step(h);
+        if (rc) return rc;
     }
     return LBF_OK;
 }
@@ -753,10 +761,17 @@ size_t handle_bytes(const lbf_params* p) {
     if (p->twocomponent) b += 2 * N * psz;
     if (half) b += 2 * N * sizeof(float);
     if (p->obstacles) b += N;
+    if (p->phi_correction) b += 3 * sizeof(double);
     return b;
 }
 
 int handle_pre_step(lbf_handle* h) { return launch_wet(h, h->cur, 1 - h->cur, false); }
+
+int handle_post_step(lbf_handle* h) {
+    if (!h->d_mass) return LBF_OK;
+    CUDA_TRY(lbf::launch_mass(h->storage, false, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass, h->stream));
+    return LBF_OK;
+}
 
 bool handle_steady(const lbf_handle* h) { return !(h->tc && h->obs && h->nwet > 0) || h->wet_pending >= 0; }
 

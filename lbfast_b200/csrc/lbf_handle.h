@@ -45,6 +45,7 @@ struct lbf_handle {
     lbf::StepLauncher launcher = nullptr;
     int zseg = 0;
     int tile_y = 8;      // rows of the kernel tile
+    double* d_mass = nullptr;  // phi correction: {sum, count, sum at the first step} (FP64)
     bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
 };
 
@@ -59,6 +60,8 @@ void handle_advance(lbf_handle* h, bool wrote_u);
 size_t handle_bytes(const lbf_params* p);
 // per-step work of h launched before its step kernel (wetting ghost update)
 int handle_pre_step(lbf_handle* h);
+// per-step work after the step kernel, on the new time level (phi mass correction)
+int handle_post_step(lbf_handle* h);
 // true when the per-step work of h repeats with period two (replayable)
 bool handle_steady(const lbf_handle* h);
 // frees the host<->device staging buffer (reallocated on the next transfer)

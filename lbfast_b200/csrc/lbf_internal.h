@@ -99,6 +99,13 @@ cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
 cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
                           const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st);
 
+// phi mass correction: initial == true stores the FP64 sum of phi over fluid
+// nodes in d_mass[2]; otherwise the sum and the count of 0.5 < phi < 0.9 go to
+// d_mass[0..1] and (d_mass[2] - sum) / count is added to those nodes.  No host
+// synchronisation (graph-capturable).
+cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
+                        cudaStream_t st);
+
 size_t storage_bytes(int storage);
 
 // sets the message returned by lbf_last_error on the calling thread

@@ -253,6 +253,67 @@ __global__ void reduce_kernel(long long N, const S* mom, const float* pres, cons
         for (int k = 0; k < 5; ++k) atomicAdd(out + k, red[k][0]);
 }
 
+// ---------------------------------------------------------------------------
+// phi mass correction (phi_sum_count_kernel + apply_lagrangian_phi_kernel,
+// lb_cuda_boundary_module.f90:459-563): FP64 sums, tree per block, one atomic
+// per block
+// ---------------------------------------------------------------------------
+template <typename SP>
+__global__ void mass_sum_kernel(long long N, const SP* phi, const int8_t* isf, double* out, bool count) {
+    double acc = 0, cnt = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        if (isf) {
+            const int f = isf[i];
+            if (f != 1 && f != -1) continue;
+        }
+        const double v = (double)phi[i];
+        acc += v;
+        if (v > 0.5 && v < 0.9) cnt += 1.0;
+    }
+    __shared__ double red[2][256];
+    red[0][threadIdx.x] = acc;
+    red[1][threadIdx.x] = cnt;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(out, red[0][0]);
+        if (count) atomicAdd(out + 1, red[1][0]);
+    }
+}
+
+template <typename SP>
+__global__ void mass_apply_kernel(long long N, SP* phi, const int8_t* isf, const double* m) {
+    if (m[1] <= 0.0) return;
+    const double corr = (m[2] - m[0]) / m[1];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        if (isf) {
+            const int f = isf[i];
+            if (f != 1 && f != -1) continue;
+        }
+        const double v = (double)phi[i];
+        if (v > 0.5 && v < 0.9) phi[i] = (SP)(v + corr);
+    }
+}
+
+cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
+                        cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(initial ? d_mass + 2 : d_mass, 0, (initial ? 1 : 2) * sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    return by_storage(storage, [&](auto tag) {
+        using SP = typename PhiStore<decltype(tag)>::type;
+        SP* f = static_cast<SP*>(phi);
+        mass_sum_kernel<SP><<<blocks_for(N, 256), 256, 0, st>>>(N, f, isf, initial ? d_mass + 2 : d_mass, !initial);
+        if (!initial) mass_apply_kernel<SP><<<blocks_for(N, 256), 256, 0, st>>>(N, f, isf, d_mass);
+        return cudaGetLastError();
+    });
+}
+
 cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
                           const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(d_out, 0, 5 * sizeof(double), st);

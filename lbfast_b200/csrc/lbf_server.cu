@@ -292,7 +292,11 @@ int issue_steps(lbf_server* s, long long nsteps) {
                 if (rc) return rc;
             }
             SRV_TRY(b.ops.launch(b.d_params[s->phase], b.d_work, b.nwork, s->stream));
-            for (Solve* v : b.members) lbf::handle_advance(v->h, v->h->dr);
+            for (Solve* v : b.members) {
+                lbf::handle_advance(v->h, v->h->dr);
+                int rc = lbf::handle_post_step(v->h);
+                if (rc) return rc;
+            }
         }
         s->phase ^= 1;
     }

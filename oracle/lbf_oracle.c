@@ -75,6 +75,7 @@ typedef struct orc_params {
     double visc1, visc2, rho_r, rho_b, sigma, width, tau_diff;
     double fx, fy, fz;
     double wettab_r;
+    int phi_correction; /* phi mass correction after every step (see mass_correction) */
 } orc_params;
 
 /* ---- lattice tables: vars_module.f90:319-338 (D3Q27) and 666-684 (D3Q19) ---- */
@@ -100,6 +101,7 @@ typedef struct orc_state {
     real *loc[2];
     real *frc[3];
     int flip;                  /* index of the buffer that is the input of the next step */
+    double phi_sum0;           /* sum of phi over fluid nodes at the first step */
     long step;
     int primed;
     /* copy_print of the last executed step (or of the primed initial state) */
@@ -814,9 +816,60 @@ static void exchange_h(orc_state *s, real **h)
 }
 
 /* Integrator preamble: integrator_module.f90:186-248 */
+/* Sum of phi over fluid nodes (|isfluid| = 1) in FP64 and the number of
+ * interface nodes 0.5 < phi < 0.9: phi_sum_count_kernel,
+ * lb_cuda_boundary_module.f90:459-506 (the initial sum as
+ * init_conditions_module.f90:468-490). */
+static double phi_sum_count(const orc_state *s, const real *ph, long *cnt)
+{
+    double sum = 0.0;
+    long c = 0;
+    int i, j, k;
+    for (k = 0; k < s->nz; k++)
+        for (j = 0; j < s->ny; j++)
+            for (i = 0; i < s->nx; i++) {
+                long n = IDX(s, i, j, k);
+                int f = s->isf[n];
+                double v;
+                if (f != 1 && f != -1) continue;
+                v = (double)ph[n];
+                sum += v;
+                if (v > 0.5 && v < 0.9) c++;
+            }
+    if (cnt) *cnt = c;
+    return sum;
+}
+
+/* phi mass correction (boundary_cds_module.f90:1864-1885 with
+ * apply_lagrangian_phi_kernel, lb_cuda_boundary_module.f90:509-563): the
+ * lost mass dphi = sum0 - sum is spread over the interface nodes,
+ * corr = dphi / count added to every fluid node with 0.5 < phi < 0.9.  The
+ * reference applies it only with open boundaries, where sum0 is corrected by
+ * the boundary fluxes; with periodic and wall boundaries those are zero.
+ * Applied here to the new phi of every step. */
+static void mass_correction(orc_state *s, real *ph)
+{
+    long cnt = 0;
+    double sum = phi_sum_count(s, ph, &cnt), corr;
+    int i, j, k;
+    if (cnt == 0) return;
+    corr = (s->phi_sum0 - sum) / (double)cnt;
+    for (k = 0; k < s->nz; k++)
+        for (j = 0; j < s->ny; j++)
+            for (i = 0; i < s->nx; i++) {
+                long n = IDX(s, i, j, k);
+                int f = s->isf[n];
+                double v;
+                if (f != 1 && f != -1) continue;
+                v = (double)ph[n];
+                if (v > 0.5 && v < 0.9) ph[n] = (real)(v + corr);
+            }
+}
+
 static void prime(orc_state *s)
 {
     real **A = s->h[s->flip];
+    if (s->p.twocomp) s->phi_sum0 = phi_sum_count(s, s->phi[s->flip], NULL);
     if (s->p.twocomp && s->p.obstacles) wetting(s, s->phi[s->flip]);
     copy_print(s, A, s->phi[s->flip]);
     if (s->p.twocomp) halo_real(s, s->phi[s->flip]);
@@ -843,6 +896,7 @@ static void one_step(orc_state *s)
     fused(s, A, B, pA);
     if (s->p.twocomp) {
         update_phi(s, A, pA, pB);
+        if (s->p.phi_correction) mass_correction(s, pB);
         halo_real(s, pB);
     }
     if (s->p.obstacles) obstacle_bb(s, A, B, pA);
