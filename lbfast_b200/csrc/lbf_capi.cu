@@ -479,64 +479,56 @@ int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype)
     if (h->obs && !h->isf_set) return fail(LBF_E_STATE, "obstacles: call lbf_set_isfluid before lbf_set_fields");
     const size_t hb = dtype == LBF_F64 ? 8 : 4;
     const long long N = h->N;
-    // 16-bit storage keeps Pi - u u (the deviation from equilibrium) with one
-    // power-of-two scale per group of fields: P, velocity, Pi - u u
-    std::vector<double> pin;  // Pi - u u, 6 x N, 16-bit modes only
     const bool half = h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16;
+    int rc = LBF_OK;
     if (half) {
-        auto at = [&](int f, long long i) -> double {
-            return dtype == LBF_F64 ? static_cast<const double*>(mom10)[f * N + i]
-                                    : (double)static_cast<const float*>(mom10)[f * N + i];
-        };
-        pin.resize(6 * (size_t)N);
-        const int ua[6] = {1, 2, 3, 1, 1, 2}, ub[6] = {1, 2, 3, 2, 3, 3};
-        double mP = 0, mU = 0, mPi = 0;
-        for (long long i = 0; i < N; ++i) {
-            double P = at(0, i);
-            if (std::isfinite(P)) mP = std::max(mP, std::fabs(P));
-            for (int f = 1; f <= 3; ++f) {
-                double v = at(f, i);
-                if (std::isfinite(v)) mU = std::max(mU, std::fabs(v));
-            }
-            for (int c = 0; c < 6; ++c) {
-                double v = at(4 + c, i) - at(ua[c], i) * at(ub[c], i);
-                pin[c * (size_t)N + i] = v;
-                if (std::isfinite(v)) mPi = std::max(mPi, std::fabs(v));
-            }
-        }
-        (void)mP;  // P is stored in FP32 in the 16-bit modes
+        // 16-bit storage keeps Pi - u u (the deviation from equilibrium) with one
+        // power-of-two scale per group of fields (velocity, Pi - u u; P stays
+        // FP32): all ten fields are staged on the device, the group maxima and
+        // Pi - u u are computed there
+        rc = ensure_staging(h, 10 * N * hb);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->staging, mom10, 10 * N * hb, cudaMemcpyHostToDevice, h->stream));
+        unsigned* d_max = reinterpret_cast<unsigned*>(h->d_red);
+        CUDA_TRY(lbf::launch_upload_maxabs(dtype, N, h->staging, d_max, h->stream));
+        unsigned bits[2];
+        CUDA_TRY(cudaMemcpyAsync(bits, d_max, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        float mU, mPi;
+        std::memcpy(&mU, &bits[0], sizeof mU);
+        std::memcpy(&mPi, &bits[1], sizeof mPi);
         h->scale[0] = 1.0;
         for (int f = 1; f <= 3; ++f) h->scale[f] = h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-2);
         for (int f = 4; f < 10; ++f) h->scale[f] = pick_scale(h->storage, mPi, 1e-4);
-    }
-    int rc = ensure_staging(h, N * hb);
-    if (rc) return rc;
-    for (int f = 0; f < 10; ++f) {
-        const char* src = static_cast<const char*>(mom10) + f * N * hb;
-        int sdt = dtype;
-        if (half && f >= 4) {
-            src = reinterpret_cast<const char*>(pin.data() + (size_t)(f - 4) * N);
-            sdt = LBF_F64;
-        }
-        const size_t sb = sdt == LBF_F64 ? 8 : 4;
-        if (sb > hb) {
-            rc = ensure_staging(h, N * sb);
-            if (rc) return rc;
-        }
-        CUDA_TRY(cudaMemcpyAsync(h->staging, src, N * sb, cudaMemcpyHostToDevice, h->stream));
-        // the host buffer of this field must not be reused before the copy ends
-        if (half && f >= 4) CUDA_TRY(cudaStreamSynchronize(h->stream));
         for (int b = 0; b < 2; ++b) {
-            char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
-            if (f == 0 && half) {
-                CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, sdt, h->pres[b], N, 1.0, h->stream));
-                continue;
-            }
-            CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, sdt, dst, N, h->scale[f], h->stream));
-            if (f >= 1 && f <= 3) {  // u_old of the first step = initial velocity (B := A)
+            CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, dtype, h->pres[b], N, 1.0, h->stream));
+            for (int f = 1; f <= 3; ++f) {
+                const char* src = static_cast<const char*>(h->staging) + f * N * hb;
+                char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
                 char* udst = static_cast<char*>(h->uold[b]) + (f - 1) * N * h->esz;
-                CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, udst, N,
+                CUDA_TRY(lbf::launch_convert_in(h->storage, false, src, dtype, dst, N, h->scale[f], h->stream));
+                CUDA_TRY(lbf::launch_convert_in(h->storage, false, src, dtype, udst, N,
                                                 h->scale[lbf::NSCALE_H - 4 + f - 1], h->stream));
+            }
+            for (int c = 0; c < 6; ++c)
+                CUDA_TRY(lbf::launch_upload_pin(h->storage, dtype, N, h->staging, c,
+                                                static_cast<char*>(h->mom[b]) + (4 + c) * N * h->esz, h->scale[4 + c],
+                                                h->stream));
+        }
+    } else {
+        rc = ensure_staging(h, N * hb);
+        if (rc) return rc;
+        for (int f = 0; f < 10; ++f) {
+            const char* src = static_cast<const char*>(mom10) + f * N * hb;
+            CUDA_TRY(cudaMemcpyAsync(h->staging, src, N * hb, cudaMemcpyHostToDevice, h->stream));
+            for (int b = 0; b < 2; ++b) {
+                char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
+                CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, dst, N, h->scale[f], h->stream));
+                if (f >= 1 && f <= 3) {  // u_old of the first step = initial velocity (B := A)
+                    char* udst = static_cast<char*>(h->uold[b]) + (f - 1) * N * h->esz;
+                    CUDA_TRY(lbf::launch_convert_in(h->storage, false, h->staging, dtype, udst, N,
+                                                    h->scale[lbf::NSCALE_H - 4 + f - 1], h->stream));
+                }
             }
         }
     }
@@ -623,27 +615,23 @@ int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype)
         return LBF_OK;
     };
     if (mom10) {
+        const bool half = is_half(h->storage);
+        double inv[lbf::NSCALE_H];
+        for (int f = 0; f < lbf::NSCALE_H; ++f) inv[f] = 1.0 / h->scale[f];
         for (int f = 0; f < 10; ++f) {
-            if (f == 0 && is_half(h->storage))
+            char* dst = static_cast<char*>(mom10) + f * N * hb;
+            if (f == 0 && half) {
                 rc = out_field(h->pres[h->cur], true, 1.0, mom10);
-            else
-                rc = out_field(static_cast<const char*>(h->mom[h->cur]) + f * N * h->esz, false, 1.0 / h->scale[f],
-                               static_cast<char*>(mom10) + f * N * hb);
+            } else if (f >= 4 && half) {
+                // stored Pi - u u: the equilibrium part is added back on the device
+                CUDA_TRY(lbf::launch_download_pi(h->storage, dtype, N, h->mom[h->cur], inv, f - 4, h->staging,
+                                                  h->stream));
+                CUDA_TRY(cudaMemcpyAsync(dst, h->staging, N * hb, cudaMemcpyDeviceToHost, h->stream));
+                CUDA_TRY(cudaStreamSynchronize(h->stream));
+            } else {
+                rc = out_field(static_cast<const char*>(h->mom[h->cur]) + f * N * h->esz, false, inv[f], dst);
+            }
             if (rc) return rc;
-        }
-        if (h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16) {
-            // stored Pi - u u: add the equilibrium part back
-            const int ua[6] = {1, 2, 3, 1, 1, 2}, ub[6] = {1, 2, 3, 2, 3, 3};
-            for (int c = 0; c < 6; ++c)
-                for (long long i = 0; i < N; ++i) {
-                    if (dtype == LBF_F64) {
-                        double* m = static_cast<double*>(mom10);
-                        m[(4 + c) * N + i] += m[ua[c] * N + i] * m[ub[c] * N + i];
-                    } else {
-                        float* m = static_cast<float*>(mom10);
-                        m[(4 + c) * N + i] += m[ua[c] * N + i] * m[ub[c] * N + i];
-                    }
-                }
         }
     }
     if (phi && h->tc) {

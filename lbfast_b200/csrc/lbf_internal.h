@@ -99,6 +99,18 @@ cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
 cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
                           const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st);
 
+// 16-bit upload, on the 10 host fields staged in device memory (f32 or f64,
+// src_dtype): the largest finite |u|, |v|, |w| and |Pi - u u| as float bits
+// in d_max[0..1], and component c (0..5) of Pi - u u converted to the storage
+// type with a scale
+cudaError_t launch_upload_maxabs(int src_dtype, long long N, const void* staged10, unsigned* d_max, cudaStream_t st);
+cudaError_t launch_upload_pin(int storage, int src_dtype, long long N, const void* staged10, int c, void* dst,
+                              double scale, cudaStream_t st);
+// 16-bit download: component c of Pi = (Pi - u u) + u u from the stored
+// fields (mom: the ten 16-bit fields, inv_scale per field) into dst (dst_dtype)
+cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const double* inv_scale,
+                               int c, void* dst, cudaStream_t st);
+
 // phi mass correction: initial == true stores the FP64 sum of phi over fluid
 // nodes in d_mass[2]; otherwise the sum and the count of 0.5 < phi < 0.9 go to
 // d_mass[0..1] and (d_mass[2] - sum) / count is added to those nodes.  No host

@@ -254,6 +254,103 @@ __global__ void reduce_kernel(long long N, const S* mom, const float* pres, cons
 }
 
 // ---------------------------------------------------------------------------
+// 16-bit upload: group maxima and Pi - u u on the device
+// ---------------------------------------------------------------------------
+constexpr int PIN_A[6] = {1, 2, 3, 1, 1, 2}, PIN_B[6] = {1, 2, 3, 2, 3, 3};
+
+template <typename T> __global__ void upload_maxabs_kernel(long long N, const T* f, unsigned* out) {
+    const int ua[6] = {1, 2, 3, 1, 1, 2}, ub[6] = {1, 2, 3, 2, 3, 3};
+    float mu = 0.f, mpi = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double m[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) m[k] = (double)f[k * N + i];
+#pragma unroll
+        for (int k = 1; k <= 3; ++k)
+            if (isfinite(m[k])) mu = fmaxf(mu, (float)fabs(m[k]));
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double v = m[4 + c] - m[ua[c]] * m[ub[c]];
+            if (isfinite(v)) mpi = fmaxf(mpi, (float)fabs(v));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = fmaxf(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+        mpi = fmaxf(mpi, __shfl_xor_sync(0xffffffffu, mpi, o));
+    }
+    // non-negative floats order as their bit patterns
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, __float_as_uint(mu));
+        atomicMax(out + 1, __float_as_uint(mpi));
+    }
+}
+
+template <typename T, typename S>
+__global__ void upload_pin_kernel(long long N, const T* f, int a, int b, int c, S* dst, float scale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const double v = (double)f[(4 + c) * N + i] - (double)f[a * N + i] * (double)f[b * N + i];
+        Codec<S>::st(dst, i, (float)v, scale);
+    }
+}
+
+cudaError_t launch_upload_maxabs(int src_dtype, long long N, const void* staged10, unsigned* d_max, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    if (src_dtype == 1)
+        upload_maxabs_kernel<double><<<blocks_for(N, 256), 256, 0, st>>>(N, static_cast<const double*>(staged10), d_max);
+    else
+        upload_maxabs_kernel<float><<<blocks_for(N, 256), 256, 0, st>>>(N, static_cast<const float*>(staged10), d_max);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_upload_pin(int storage, int src_dtype, long long N, const void* staged10, int c, void* dst,
+                              double scale, cudaStream_t st) {
+    auto go = [&](auto stag) {
+        using S = decltype(stag);
+        if (src_dtype == 1)
+            upload_pin_kernel<double, S><<<blocks_for(N, 256), 256, 0, st>>>(
+                N, static_cast<const double*>(staged10), PIN_A[c], PIN_B[c], c, static_cast<S*>(dst), (float)scale);
+        else
+            upload_pin_kernel<float, S><<<blocks_for(N, 256), 256, 0, st>>>(
+                N, static_cast<const float*>(staged10), PIN_A[c], PIN_B[c], c, static_cast<S*>(dst), (float)scale);
+        return cudaGetLastError();
+    };
+    if (storage == 1) return go(__half());
+    if (storage == 2) return go(__nv_bfloat16());
+    return cudaErrorInvalidValue;
+}
+
+template <typename S, typename T>
+__global__ void download_pi_kernel(long long N, const S* m, float sa, float sb, float sc, int a, int b, int c, T* dst) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const double ua = (double)Codec<S>::ld(m + a * N, i, sa);
+        const double ub = (double)Codec<S>::ld(m + b * N, i, sb);
+        const double pn = (double)Codec<S>::ld(m + (4 + c) * N, i, sc);
+        dst[i] = (T)(pn + ua * ub);
+    }
+}
+
+cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const double* inv_scale,
+                               int c, void* dst, cudaStream_t st) {
+    const int a = PIN_A[c], b = PIN_B[c];
+    auto go = [&](auto stag) {
+        using S = decltype(stag);
+        const S* m = static_cast<const S*>(mom);
+        if (dst_dtype == 1)
+            download_pi_kernel<S, double><<<blocks_for(N, 256), 256, 0, st>>>(
+                N, m, (float)inv_scale[a], (float)inv_scale[b], (float)inv_scale[4 + c], a, b, c, static_cast<double*>(dst));
+        else
+            download_pi_kernel<S, float><<<blocks_for(N, 256), 256, 0, st>>>(
+                N, m, (float)inv_scale[a], (float)inv_scale[b], (float)inv_scale[4 + c], a, b, c, static_cast<float*>(dst));
+        return cudaGetLastError();
+    };
+    if (storage == 1) return go(__half());
+    if (storage == 2) return go(__nv_bfloat16());
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
 // phi mass correction (phi_sum_count_kernel + apply_lagrangian_phi_kernel,
 // lb_cuda_boundary_module.f90:459-563): FP64 sums, tree per block, one atomic
 // per block
