@@ -49,7 +49,7 @@ B_LUP = {"f32": 112, "f16": 64, "bf16": 64, "f64": 224}  # algorithmic bytes per
 # DRAM bytes (read + write) of one step launch from one ncu capture at this
 # workload: profiles/stream_kernel_laplace256_f32.md and
 # profiles/stream_kernel_laplace256_full.md
-NCU_TRAFFIC = {("f32", 256): 1886000000}
+NCU_TRAFFIC = {("f32", 256): 1844577280}
 
 
 def workload(storage: str = "f32", L: int = LBOX):
