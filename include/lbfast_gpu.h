@@ -212,8 +212,19 @@ typedef struct lbf_run {
  * and run are first set to the DOBENCHMARK defaults.  The compile-time macro
  * fields of p (lattice, highorder, twocomponent, densratio, obstacles,
  * storage, printphi) are left as the caller set them.  Unknown keys,
- * malformed values, openbc = 1 and lrestart = .true. are errors. */
+ * malformed values and openbc = 1 are errors. */
 int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run);
+
+/* The reference's restart file <dir>/restart.raw (write_restart_serial_2c /
+ * _1c and their readers, print_module.f90:1030-1677): one time level in
+ * float32, the ten moments in the reference's file order (P, u, v, w, Pxx,
+ * Pxy, Pxz, Pyy, Pyz, Pzz), phi when phi != NULL (two components), then iframe
+ * and iframe2D (int32).  mom10 is in this header's order (P, u, v, w, Pxx, Pyy,
+ * Pzz, Pxy, Pxz, Pyz), Fortran order.  The reader checks the file size. */
+int lbf_write_restart_raw(const char* dir, int lx, int ly, int lz, const float* mom10, const float* phi, int iframe,
+                          int iframe2D);
+int lbf_read_restart_raw(const char* dir, int lx, int ly, int lz, float* mom10, float* phi, int* iframe,
+                         int* iframe2D);
 
 /* raw + XDMF writer of print_raw_sync (print_module.f90:2007-2180): writes
  * <dir>/out_rho_NNNNNN.raw/.xdmf, out_vel_..., and out_press_... when press

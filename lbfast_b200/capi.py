@@ -26,7 +26,8 @@ EXPORTED = (
     "lbf_set_fields", "lbf_step", "lbf_sync", "lbf_get_step", "lbf_get_fields", "lbf_get_print_fields",
     "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
     "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
-    "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning",
+    "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning", "lbf_write_restart_raw",
+    "lbf_read_restart_raw",
 )
 SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -92,6 +93,8 @@ def load() -> C.CDLL:
     lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
     lib.lbf_ic_droplet.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
     lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    lib.lbf_write_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, C.c_int, C.c_int]
+    lib.lbf_read_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, P(C.c_int), P(C.c_int)]
     lib.lbf_server_create.argtypes = [P(LbfServerConfig), P(vp)]
     lib.lbf_server_destroy.argtypes = [vp]
     lib.lbf_server_submit.argtypes = [vp, P(LbfParams), i8p, vp, vp, C.c_int, C.c_longlong, P(C.c_longlong)]
@@ -378,6 +381,26 @@ def ic_droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio
                                 float(rho_r), float(rho_b), int(densratio), _ptr(i, C.c_int8),
                                 _ptr(m, C.c_double), _ptr(phi, C.c_double)))
     return m, phi
+
+
+def write_restart_raw(directory: str, mom10: np.ndarray, phi: np.ndarray | None = None, iframe: int = 0,
+                      iframe2D: int = 0) -> None:
+    """The reference's restart.raw (float32, one time level) in `directory`."""
+    _, lz, ly, lx = mom10.shape
+    m = np.ascontiguousarray(mom10, dtype=np.float32)
+    p = None if phi is None else np.ascontiguousarray(phi, dtype=np.float32)
+    check(load().lbf_write_restart_raw(directory.encode(), lx, ly, lz, _ptr(m, C.c_float), _ptr(p, C.c_float),
+                                       int(iframe), int(iframe2D)))
+
+
+def read_restart_raw(directory: str, lx: int, ly: int, lz: int, twocomponent: bool):
+    """(mom10, phi or None, iframe, iframe2D) from `directory`/restart.raw."""
+    m = np.empty((10, lz, ly, lx), dtype=np.float32)
+    p = np.empty((lz, ly, lx), dtype=np.float32) if twocomponent else None
+    fr, fr2 = C.c_int(), C.c_int()
+    check(load().lbf_read_restart_raw(directory.encode(), lx, ly, lz, _ptr(m, C.c_float), _ptr(p, C.c_float),
+                                      C.byref(fr), C.byref(fr2)))
+    return m, p, fr.value, fr2.value
 
 
 def write_raw_xdmf(directory: str, iframe: int, rho, vel, press=None) -> None:

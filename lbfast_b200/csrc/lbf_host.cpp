@@ -429,9 +429,58 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
         std::fprintf(stderr, "lbf_read_namelists: openbc = %d: open boundaries are not supported\n", run->openbc);
         return LBF_E_UNSUPPORTED;
     }
-    if (run->lrestart) {
-        std::fprintf(stderr, "lbf_read_namelists: lrestart: restart files are not supported\n");
-        return LBF_E_UNSUPPORTED;
-    }
+    return LBF_OK;
+}
+
+// ---- restart.raw (print_module.f90:1030-1474 and 1474-1677) ----
+// The reference's restart is one time level in float32, stream-unformatted:
+// the ten moment fields in the order of its hfields indices 1,2,3,4,5,8,9,6,10,7
+// (P, u, v, w, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz), then phi for two components, then
+// iframe and iframe2D as int32.  mom10 here is ordered P, u, v, w, Pxx, Pyy,
+// Pzz, Pxy, Pxz, Pyz.
+namespace {
+const int kRestartOrder[10] = {0, 1, 2, 3, 4, 7, 8, 5, 9, 6};
+
+std::string restart_path(const char* dir) {
+    std::string d = dir ? dir : ".";
+    if (!d.empty() && d.back() != '/') d += '/';
+    return d + "restart.raw";
+}
+}  // namespace
+
+int lbf_write_restart_raw(const char* dir, int lx, int ly, int lz, const float* mom10, const float* phi, int iframe,
+                          int iframe2D) {
+    if (!mom10 || lx < 1 || ly < 1 || lz < 1) return LBF_E_ARG;
+    const long long N = (long long)lx * ly * lz;
+    std::FILE* f = std::fopen(restart_path(dir).c_str(), "wb");
+    if (!f) return LBF_E_IO;
+    bool ok = true;
+    for (int k = 0; k < 10 && ok; ++k) ok = std::fwrite(mom10 + kRestartOrder[k] * N, sizeof(float), N, f) == (size_t)N;
+    if (ok && phi) ok = std::fwrite(phi, sizeof(float), N, f) == (size_t)N;
+    const int32_t fr[2] = {iframe, iframe2D};
+    if (ok) ok = std::fwrite(fr, sizeof(int32_t), 2, f) == 2;
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? LBF_OK : LBF_E_IO;
+}
+
+int lbf_read_restart_raw(const char* dir, int lx, int ly, int lz, float* mom10, float* phi, int* iframe,
+                         int* iframe2D) {
+    if (!mom10 || lx < 1 || ly < 1 || lz < 1) return LBF_E_ARG;
+    const long long N = (long long)lx * ly * lz;
+    std::FILE* f = std::fopen(restart_path(dir).c_str(), "rb");
+    if (!f) return LBF_E_IO;
+    std::fseek(f, 0, SEEK_END);
+    const long long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    const long long want = (long long)sizeof(float) * N * (phi ? 11 : 10) + 8;
+    bool ok = size == want;
+    for (int k = 0; k < 10 && ok; ++k) ok = std::fread(mom10 + kRestartOrder[k] * N, sizeof(float), N, f) == (size_t)N;
+    if (ok && phi) ok = std::fread(phi, sizeof(float), N, f) == (size_t)N;
+    int32_t fr[2] = {0, 0};
+    if (ok) ok = std::fread(fr, sizeof(int32_t), 2, f) == 2;
+    std::fclose(f);
+    if (!ok) return LBF_E_IO;
+    if (iframe) *iframe = fr[0];
+    if (iframe2D) *iframe2D = fr[1];
     return LBF_OK;
 }

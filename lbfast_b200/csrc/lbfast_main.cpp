@@ -170,6 +170,20 @@ int main(int argc, char** argv) {
         }
     }
 
+    // ---- restart: integrator_module.f90:167-176 (replaces the initial fields) ----
+    int iframe = 0, iframe2D = 0;
+    if (run.lrestart) {
+        std::vector<float> m32(10 * N), p32(N);
+        if (lbf_read_restart_raw("output", lx, ly, lz, m32.data(), p.twocomponent ? p32.data() : nullptr, &iframe,
+                                 &iframe2D) != LBF_OK) {
+            std::fprintf(stderr, "ERROR: unable to read the file: output/restart.raw\n");
+            return 1;
+        }
+        std::copy(m32.begin(), m32.end(), mom.begin());
+        if (p.twocomponent) std::copy(p32.begin(), p32.end(), phi.begin());
+        std::printf("restart read: iframe %d\n", iframe);
+    }
+
     lbf_handle* h = nullptr;
     CHECK(lbf_create(&p, &h));
     if (p.obstacles) CHECK(lbf_set_isfluid(h, isf.data()));
@@ -178,11 +192,10 @@ int main(int argc, char** argv) {
     // ---- output set-up: print_module.f90:277-445 ----
     std::vector<float> rho(N), vel(3 * N), press(N);
     const bool do_raw = run.lprint && run.lraw;
-    if (do_raw) mkdir("output", 0755);
-    int iframe = 0;
+    if (do_raw || run.lwriterestart) mkdir("output", 0755);
     if (run.lvtk) std::fprintf(stderr, "lbfast: lvtk ignored (VTK output is not provided)\n");
     if (run.nplanes > 0) std::fprintf(stderr, "lbfast: nplanes ignored (2-D plane output is not provided)\n");
-    if (run.lprint) {
+    if (run.lprint && !run.lrestart) {
         CHECK(lbf_get_print_fields(h, rho.data(), vel.data(), press.data()));
         if (do_raw)
             CHECK(lbf_write_raw_xdmf("output", iframe, lx, ly, lz, rho.data(), vel.data(),
@@ -220,6 +233,7 @@ int main(int argc, char** argv) {
             double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             if (el > run.time_limit) {
                 std::printf("Time limit %16.2f sec reached at step %16d after %16.2f sec\n", run.time_limit, step, el);
+                run.lwriterestart = 1;  // integrator_module.f90:819
                 break;
             }
         }
@@ -229,6 +243,13 @@ int main(int argc, char** argv) {
     double glups = (double)lx * ly * lz * (double)run.nsteps / tot * 1e-9;  // LBFAST.f90:499-500
     double sums[5];
     CHECK(lbf_reduce(h, sums));
+    // ---- write restart: integrator_module.f90:834-840 ----
+    if (run.lwriterestart) {
+        std::vector<float> m32(10 * N), p32(N);
+        CHECK(lbf_get_fields(h, m32.data(), p.twocomponent ? p32.data() : nullptr, nullptr, LBF_F32));
+        CHECK(lbf_write_restart_raw("output", lx, ly, lz, m32.data(), p.twocomponent ? p32.data() : nullptr, iframe,
+                                    iframe2D));
+    }
     std::printf(" time elapsed: %g s\n", tot);
     std::printf(" glups: %g\n", glups);
     std::printf(" sums (phi, P, u, v, w): %.12g %.12g %.12g %.12g %.12g\n", sums[0], sums[1], sums[2], sums[3], sums[4]);

@@ -182,3 +182,49 @@ def test_phi_mass_correction_holds_the_sum(storage, bar):
     s0 = float(np.sum(phi))
     assert abs(sums[1] - s0) / s0 < bar, sums
     assert abs(sums[0] - s0) / s0 > 1e-4, sums
+
+
+def test_restart_resumes_the_run(tmp_path):
+    """A run stopped after 20 steps, written to restart.raw and resumed stays
+    within 1e-3 rel-L2 of the uninterrupted 40-step run.  The restart is the
+    reference's (print_module.f90:1474-1677): one time level in float32, so the
+    resumed run starts from rounded fields and from u_old = u."""
+    p, isf, m, phi = make_case("q27ho_2c_dr", "f32")
+    a = L.Solver(p)
+    a.set_fields(m, phi)
+    a.step(40)
+    ma, pa, _ = a.get_fields()
+    a.close()
+    b = L.Solver(p)
+    b.set_fields(m, phi)
+    b.step(20)
+    mb, pb, _ = b.get_fields(np.float32)
+    b.close()
+    L.write_restart_raw(str(tmp_path), mb, pb, 1, 0)
+    m2, p2, fr, _ = L.read_restart_raw(str(tmp_path), p.lx, p.ly, p.lz, True)
+    assert fr == 1
+    c = L.Solver(p)
+    c.set_fields(m2, p2)
+    c.step(20)
+    mc, pc, _ = c.get_fields()
+    c.close()
+    assert rel_l2(mc, ma) < 1e-3 and rel_l2(pc, pa) < 1e-4, (rel_l2(mc, ma), rel_l2(pc, pa))
+
+
+def test_driver_writes_and_reads_restart(tmp_path):
+    """lwriterestart writes output/restart.raw at the end of the run
+    (integrator_module.f90:834-840); lrestart resumes from it with the frame
+    counter restored (integrator_module.f90:167-176)."""
+    exe = os.path.join(ROOT, "lbfast_b200", "_lib", "lbfast")
+    text = open(os.path.join(ROOT, "tests", "golden", "channel.inp")).read()
+    flags = ["-DLATTICE=27", "-DHIGHORDER", "-DTWOCOMPONENT", "-DDENSRATIO", "-DINTERNAL_OBSTACLES", "-DPRINTPHI"]
+    (tmp_path / "a.inp").write_text(text.replace("   nsteps=40", "   nsteps=40\n   lwriterestart=.true."))
+    r = subprocess.run([exe, *flags, "a.inp"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    n = 36 * 20 * 24
+    assert (tmp_path / "output" / "restart.raw").stat().st_size == 4 * n * 11 + 8
+    (tmp_path / "b.inp").write_text(text.replace("   nsteps=40", "   nsteps=20\n   lrestart=.true."))
+    r = subprocess.run([exe, *flags, "b.inp"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "restart read: iframe 2" in r.stdout
+    assert (tmp_path / "output" / "out_rho_000003.raw").exists()

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from cases import _spheres_solid
+import lbfast_b200 as L
 from lbfast_b200 import capi
 from oracle import oracle as O
 
@@ -146,3 +147,29 @@ def test_create_rejects_invalid_parameters_before_device_work(bad):
     rc = capi.load().lbf_create(C.byref(p), C.byref(h))
     assert rc in (-1, -5) and not h
     assert capi.last_error()
+
+
+@pytest.mark.parametrize("two", [True, False])
+def test_restart_file_layout_and_round_trip(tmp_path, two):
+    """restart.raw as print_module.f90:1474-1677 writes it: float32 moments in
+    the reference's hfields order 1,2,3,4,5,8,9,6,10,7, phi (two components),
+    then iframe and iframe2D; the reader restores the header's order."""
+    lx, ly, lz = 6, 5, 4
+    rng = np.random.default_rng(3)
+    m = rng.standard_normal((10, lz, ly, lx)).astype(np.float32)
+    phi = rng.random((lz, ly, lx)).astype(np.float32) if two else None
+    L.write_restart_raw(str(tmp_path), m, phi, 17, 3)
+    raw = np.fromfile(tmp_path / "restart.raw", dtype=np.uint8)
+    n = lx * ly * lz
+    assert raw.size == 4 * n * (11 if two else 10) + 8
+    f = raw[: 4 * n * (11 if two else 10)].view(np.float32).reshape(-1, lz, ly, lx)
+    assert np.array_equal(f[:10], m[[0, 1, 2, 3, 4, 7, 8, 5, 9, 6]])
+    if two:
+        assert np.array_equal(f[10], phi)
+    assert list(raw[-8:].view(np.int32)) == [17, 3]
+    m2, p2, fr, fr2 = L.read_restart_raw(str(tmp_path), lx, ly, lz, two)
+    assert np.array_equal(m2, m) and (fr, fr2) == (17, 3)
+    if two:
+        assert np.array_equal(p2, phi)
+    with pytest.raises(L.LbfError):  # size check: a one-component file is not a two-component restart
+        L.read_restart_raw(str(tmp_path), lx, ly, lz, not two)
