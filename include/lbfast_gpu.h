@@ -71,15 +71,19 @@ typedef struct lbf_params {
     int zseg;                /* planes per z segment of the kernel (one CTA per tile and segment); 0 = a
                                 persistent schedule: one CTA per resident slot, each advancing an equal
                                 contiguous share of the box's columns x planes */
-    int tile_y;              /* rows of the kernel's 32-wide tile: 8 or 16 (FP64: 8 only); 0 = autotuned
-                                together with zseg (when zseg = 0) at the first lbf_step: each candidate
-                                (tile, zseg) is timed on the box itself, the fastest is kept and remembered
-                                for boxes of the same shape and class.  Results do not depend on either. */
+    int tile_y;              /* rows of the kernel's 32-wide tile: 8 or 16 (FP64: 8 only).  0 = 16 rows (8 in
+                                FP64) and, when zseg = 0, the schedule autotuned at the first lbf_step: each
+                                candidate (persistent, z segments of several lengths) is timed on the box
+                                itself, the fastest is kept and remembered for boxes of the same shape and
+                                class.  The schedule does not change the results; the tile height may in
+                                the last bit (separate compilations). */
     int phi_correction;      /* two components: after every step restore the FP64 sum of phi over fluid
                                 nodes to its value at the first step by adding (sum0 - sum) / count to
                                 the count interface nodes with 0.5 < phi < 0.9 (the reference's
                                 BCPHIFLUX Lagrange correction, boundary_cds_module.f90:1864-1885, which it
                                 applies with open boundaries only); 0 = off (the reference default) */
+    int smagorinsky;         /* SMAGORINSKI: LES relaxation time from the non-equilibrium stress
+                                (lb_cuda_fused_module.f90:609-616, lb_cuda_boundary_module.f90:150-160) */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;

@@ -42,6 +42,7 @@ class LbfParams(C.Structure):
         ("sigma", C.c_double), ("width", C.c_double), ("tau_diff", C.c_double),
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
         ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int), ("phi_correction", C.c_int),
+        ("smagorinsky", C.c_int),
     ]
 
 
@@ -159,6 +160,7 @@ class Params:
     zseg: int = 0
     tile_y: int = 0
     phi_correction: int = 0
+    smagorinsky: int = 0
 
     def to_c(self) -> LbfParams:
         p = LbfParams()

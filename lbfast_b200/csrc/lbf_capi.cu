@@ -101,11 +101,16 @@ int auto_zseg(int nx, int ny, int nz, int tile_y) {
     return zseg;
 }
 
-// ---- autotuner of the tile height and z segment ----
-// Every candidate launch steps the current time level into the other buffer
-// set, which the next real step overwrites, so timing on the box's own fields
-// leaves its state unchanged (wetting, which changes host-side state, is not
-// part of a trial).  The winner is remembered per box shape and class.
+// ---- autotuner of the schedule ----
+// The tile height is fixed per storage (default_tile): kernels of different
+// tile heights are different compilations whose floating-point contractions
+// may differ in the last bit, while one kernel gives the same bits for every
+// z segmentation and schedule -- so the tuned result is reproducible from run
+// to run whatever the timings.  Every candidate launch steps the current time
+// level into the other buffer set, which the next real step overwrites, so
+// timing on the box's own fields leaves its state unchanged (wetting, which
+// changes host-side state, is not part of a trial).  The winner is remembered
+// per box shape and class.
 struct TuneKey {
     int v[12];
     bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 12, o.v, o.v + 12); }
@@ -136,8 +141,7 @@ int autotune(lbf_handle* h) {
         }
     }
     std::vector<std::pair<int, int>> cand;
-    for (int ty : {8, 16}) {
-        if (!lbf::tile_available(h->storage, ty)) continue;
+    for (int ty : {h->tile_y}) {
         std::vector<int> zs;
         if (h->p.zseg > 0) {
             zs.push_back(std::min(h->p.zseg, h->nz));
@@ -327,7 +331,9 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "tile of %d rows not built for this storage", p->tile_y);
     }
-    h->tile_y = p->tile_y ? p->tile_y : 8;
+    // rows of the tile: the one requested, else 16 (8 in FP64, whose rings of
+    // 16 rows do not fit in shared memory); tile_y = 0 also tunes the schedule
+    h->tile_y = p->tile_y ? p->tile_y : (lbf::tile_available(p->storage, 16) ? 16 : 8);
     h->tuned = p->tile_y != 0;
     h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, p->twocomponent, h->tile_y);
     if (!h->launcher) {
@@ -716,7 +722,7 @@ void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u) {
     const int in = h->cur, out = 1 - h->cur;
     a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
     a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
-    a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg;
+    a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg; a.smag = h->p.smagorinsky;
     a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
     a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
     a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;

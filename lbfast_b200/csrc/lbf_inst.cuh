@@ -17,7 +17,7 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.pbx = a.pbx; p.pby = a.pby; p.pbz = a.pbz;
     p.plane = (long long)a.nx * a.ny;
     p.N = p.plane * a.nz;
-    p.densratio = a.densratio; p.obstacles = a.obstacles; p.write_u = a.write_u;
+    p.densratio = a.densratio; p.obstacles = a.obstacles; p.write_u = a.write_u; p.smag = a.smag;
     p.zseg = a.zseg;
     p.omega = (R)a.omega; p.visc1 = (R)a.visc1; p.visc2 = (R)a.visc2;
     p.rho_r = (R)a.rho_r; p.rho_b = (R)a.rho_b; p.beta = (R)a.beta; p.kapp = (R)a.kapp;

@@ -11,7 +11,7 @@ constexpr int NSCALE_H = 14;
 // Storage-agnostic arguments of one fused step launch.
 struct StepArgs {
     int nx, ny, nz, pbx, pby, pbz;
-    int densratio, obstacles, write_u, zseg;
+    int densratio, obstacles, write_u, zseg, smag;
     double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     double scale[NSCALE_H];
     const void* min;

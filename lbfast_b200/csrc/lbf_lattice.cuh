@@ -114,7 +114,7 @@ template <typename S, typename R> struct StepParams {
     int pbx, pby, pbz;
     long long plane;  // nx*ny
     long long N;      // nx*ny*nz
-    int densratio, obstacles, write_u;
+    int densratio, obstacles, write_u, smag;
     int zseg;         // planes per z segment
     R omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     R scale[NSCALE], inv_scale[NSCALE];

@@ -50,6 +50,9 @@ template <int BYTES> __device__ __forceinline__ void cp_async(void* smem, const 
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Smagorinsky constant of the reference: the single-precision product 0.053 * 18.0
+constexpr double SMAG_C = (double)(0.053f * 18.0f);
+
 // fields staged per collision node: 10 moments (+3 u_old with a density ratio)
 constexpr int NSTAGE = 13;
 
@@ -471,6 +474,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     fxv = p.fx; fyv = p.fy; fzv = p.fz;
                 }
                 R grx = 0, gry = 0, grz = 0, cv = 0, omega;
+                R visc_l = p.visc1;  // local viscosity (mixture with two components)
                 if constexpr (TC) {
                     const R chem = R(4) * p.beta * phi * (phi - R(1)) * (phi - R(0.5)) - p.kapp * lap;
                     fxv += chem * gfx;
@@ -496,6 +500,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     const R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
                     const R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
                     const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
+                    visc_l = visc;
                     omega = rcp<R>(visc * R(3) + R(0.5));
                     // mask * visc / (tau cs^2), with 1/tau = omega
                     cv = mask * visc * omega * R(3);
@@ -517,6 +522,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     w += R(0.5) * fzv * inv;
                     if constexpr (TC) {
                         const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
+                        visc_l = visc;
                         omega = rcp<R>(visc * R(3) + R(0.5));
                     } else {
                         omega = p.omega;
@@ -553,6 +559,15 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 const R Xn = pxx - u * u, Yn = pyy - v * v, Zn = pzz - w * w;
                 const R XYn = pxy - u * v, XZn = pxz - u * w, YZn = pyz - v * w;
                 const R Fx = tfx * inv, Fy = tfy * inv, Fz = tfz * inv;
+                if (p.smag) {
+                    // SMAGORINSKI (lb_cuda_fused_module.f90:609-616): relaxation time from the
+                    // Frobenius norm of the non-equilibrium stress; the moments prologue above
+                    // keeps the molecular one, as the reference's moments kernel does
+                    const R QQ = Xn * Xn + Yn * Yn + Zn * Zn + R(2) * (XYn * XYn + XZn * XZn + YZn * YZn);
+                    const R v3 = R(3) * visc_l;
+                    const R tau = R(0.5) + R(1.0 / 6.0) * (v3 + sqrt_a<R>(v3 * v3 + R(SMAG_C) * sqrt_a<R>(R(2) * QQ) * inv));
+                    omega = rcp<R>(tau);
+                }
                 sP = P;
                 spxx = Xn; spyy = Yn; spzz = Zn; spxy = XYn; spxz = XZn; spyz = YZn; som = omega;
                 const R om1 = R(1) - omega;
@@ -768,17 +783,25 @@ __device__ __forceinline__ void run_share(const int nx, const int ny, const int 
 // cut into gridDim.x equal contiguous shares (a share may end inside one
 // column and continue at the bottom of the next), so every CTA does the same
 // work and pays the pipeline fill of a segment start only once or twice.
+// Both schedules are expressed as a range of column-planes walked by ONE call
+// site of step_body, so the kernel holds a single compiled copy of the step:
+// separately inlined copies may contract floating-point operations
+// differently and give results that differ in the last bit.
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
+    long long s0, s1;
     if (p.zseg > 0) {
+        const long long col = (long long)blockIdx.y * ((p.nx + TX - 1) / TX) + blockIdx.x;
         const int z0 = blockIdx.z * p.zseg;
-        step_body<LAT, HO, TC, S, R, TYV>(p, blockIdx.x, blockIdx.y, z0, min(z0 + p.zseg, p.nz));
-        return;
+        s0 = col * p.nz + z0;
+        s1 = s0 + min(p.zseg, p.nz - z0);
+    } else {
+        const long long W = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV) * p.nz;
+        const long long share = (W + gridDim.x - 1) / gridDim.x;
+        s0 = (long long)blockIdx.x * share;
+        s1 = min(W, s0 + share);
     }
-    const long long W = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV) * p.nz;
-    const long long share = (W + gridDim.x - 1) / gridDim.x;
-    const long long s0 = (long long)blockIdx.x * share;
-    run_share<TYV>(p.nx, p.ny, p.nz, s0, min(W, s0 + share),
+    run_share<TYV>(p.nx, p.ny, p.nz, s0, s1,
                    [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV>(p, bx, by, z0, z1); });
 }
 

@@ -2,7 +2,7 @@
 // C ABI (include/lbfast_gpu.h).
 //
 //   lbfast [-DLATTICE=19|27] [-DHIGHORDER] [-DTWOCOMPONENT] [-DDENSRATIO]
-//          [-DINTERNAL_OBSTACLES] [-DWETTABILITY] [-DPRINTPHI] [-DWRITEPRESS]
+//          [-DINTERNAL_OBSTACLES] [-DWETTABILITY] [-DPRINTPHI] [-DWRITEPRESS] [-DSMAGORINSKI]
 //          [-DTAYLORGREEN|-DLAPLACE|-DLAMBTEST] [--storage=f32|f16|bf16|f64]
 //          input.inp
 //
@@ -33,7 +33,7 @@ namespace {
 struct Flags {
     int lattice = 27;
     bool highorder = false, twocomponent = false, densratio = false, obstacles = false;
-    bool printphi = false, writepress = false, wettability = false;
+    bool printphi = false, writepress = false, wettability = false, smagorinsky = false;
     bool taylorgreen = false, laplace = false, lambtest = false;
     int storage = LBF_STORE_F32;
     std::string input;
@@ -71,6 +71,7 @@ Flags parse_flags(int argc, char** argv) {
         else if (a == "-DDENSRATIO") fl.densratio = true;
         else if (a == "-DINTERNAL_OBSTACLES") fl.obstacles = true;
         else if (a == "-DWETTABILITY") fl.wettability = true;
+        else if (a == "-DSMAGORINSKI") fl.smagorinsky = true;
         else if (a == "-DPRINTPHI") fl.printphi = true;
         else if (a == "-DWRITEPRESS") fl.writepress = true;
         else if (a == "-DTAYLORGREEN") fl.taylorgreen = true;
@@ -113,6 +114,7 @@ int main(int argc, char** argv) {
     p.obstacles = fl.obstacles;
     p.storage = fl.storage;
     p.printphi = fl.printphi;
+    p.smagorinsky = fl.smagorinsky;
     p.visc2 = 0.0;
     p.wettab_r = 90.0;
     lbf_run run;

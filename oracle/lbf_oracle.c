@@ -76,6 +76,7 @@ typedef struct orc_params {
     double fx, fy, fz;
     double wettab_r;
     int phi_correction; /* phi mass correction after every step (see mass_correction) */
+    int smagorinsky;    /* SMAGORINSKI LES relaxation time (see smag_omega) */
 } orc_params;
 
 /* ---- lattice tables: vars_module.f90:319-338 (D3Q27) and 666-684 (D3Q19) ---- */
@@ -584,6 +585,20 @@ static void moments(orc_state *s, real **hs, real **ho, const real *ph)
 }
 
 /* Post-collision population f*_l at node c: lb_cuda_fused_module.f90:531-713 */
+/* SMAGORINSKI (lb_cuda_fused_module.f90:609-616, lb_cuda_boundary_module.f90:150-160):
+ * tau = 1/2 + (3 nu + sqrt((3 nu)^2 + 0.053*18 sqrt(2 Q) / rho_phi)) / 6 with Q the
+ * squared Frobenius norm of the non-equilibrium stress; 0.053*18 is a
+ * single-precision product in the reference. */
+static real smag_omega(real visc, real pxx, real pyy, real pzz, real pxy, real pxz, real pyz, real invrho)
+{
+    const real QQ = pxx * pxx + pyy * pyy + pzz * pzz + (real)2.0 * (pxy * pxy + pxz * pxz + pyz * pyz);
+    const real c = (real)(double)(0.053f * 18.0f);
+    real tau = (real)0.5 + ((real)1.0 / (real)6.0) *
+                               ((real)3.0 * visc + (real)sqrt(((real)3.0 * visc) * ((real)3.0 * visc) +
+                                                              c * (real)sqrt((real)2.0 * QQ) * invrho));
+    return (real)1.0 / tau;
+}
+
 static void collide_node(const orc_state *s, real **hin, const real *ph, long c, real *fout)
 {
     const int tc = s->p.twocomp, dr = s->p.densratio;
@@ -601,14 +616,15 @@ static void collide_node(const orc_state *s, real **hin, const real *ph, long c,
     }
     pxx = pxx - u * u; pyy = pyy - v * v; pzz = pzz - w * w;
     pxy = pxy - u * v; pxz = pxz - u * w; pyz = pyz - v * w;
-    real om;
+    real om, visc = s->visc1;
     if (tc) {
-        real visc = (s->rho_r * s->visc1 * phi + (ONE - phi) * s->visc2 * s->rho_b) * inv;
+        visc = (s->rho_r * s->visc1 * phi + (ONE - phi) * s->visc2 * s->rho_b) * inv;
         om = visc * invcssq + (real)0.5;
         om = (real)1.0 / om;
     } else {
         om = s->omega;
     }
+    if (s->p.smagorinsky) om = smag_omega(visc, pxx, pyy, pzz, pxy, pxz, pyz, inv);
     const real (*Mi)[27] = s->minv;
     real uu = HALF * (u * u + v * v + w * w) * invcssq;
     real feq = s->w[0] * (press - uu);
@@ -758,14 +774,15 @@ static void obstacle_bb(orc_state *s, real **hin, real **hout, const real *ph)
                 real pxy = hin[7][c] - u * v, pxz = hin[8][c] - u * w, pyz = hin[9][c] - v * w;
                 real o[10];
                 for (l = 0; l < 10; l++) o[l] = hout[l][c];
-                real om;
+                real om, visc = s->visc1;
                 if (tc) {
-                    real visc = (s->rho_r * s->visc1 * phi + (ONE - phi) * s->visc2 * s->rho_b) / rhophi;
+                    visc = (s->rho_r * s->visc1 * phi + (ONE - phi) * s->visc2 * s->rho_b) / rhophi;
                     om = visc * (real)3.0 + (real)0.5;
                     om = (real)1.0 / om;
                 } else {
                     om = s->omega;
                 }
+                if (s->p.smagorinsky) om = smag_omega(visc, pxx, pyy, pzz, pxy, pxz, pyz, (real)1.0 / rhophi);
                 for (l = 1; l < s->nl; l++) {
                     int lo = s->opp[l];
                     if (s->isf[IDX(s, i + s->ex[lo], j + s->ey[lo], k + s->ez[lo])] != 0) continue;

@@ -31,7 +31,7 @@ class OrcParams(C.Structure):
         ("visc1", C.c_double), ("visc2", C.c_double), ("rho_r", C.c_double),
         ("rho_b", C.c_double), ("sigma", C.c_double), ("width", C.c_double),
         ("tau_diff", C.c_double), ("fx", C.c_double), ("fy", C.c_double),
-        ("fz", C.c_double), ("wettab_r", C.c_double), ("phi_correction", C.c_int),
+        ("fz", C.c_double), ("wettab_r", C.c_double), ("phi_correction", C.c_int), ("smagorinsky", C.c_int),
     ]
 
 
@@ -87,7 +87,7 @@ def set_threads(n: int) -> None:
 
 PARAM_KEYS = ("lx", "ly", "lz", "pbc_x", "pbc_y", "pbc_z", "lattice", "highorder",
               "twocomp", "densratio", "obstacles", "visc1", "visc2", "rho_r", "rho_b",
-              "sigma", "width", "tau_diff", "fx", "fy", "fz", "wettab_r", "phi_correction")
+              "sigma", "width", "tau_diff", "fx", "fy", "fz", "wettab_r", "phi_correction", "smagorinsky")
 
 
 class Oracle:

@@ -56,11 +56,13 @@ def _spheres_solid(rng, shape, n, rmin, rmax):
 
 
 def make_case(name: str, storage: str = "f32"):
-    if name.endswith("_corr"):
-        # the same case with the phi mass correction after every step
-        p, isf, m, phi = make_case(name[:-5], storage)
-        p.phi_correction = 1
-        return p, isf, m, phi
+    for suffix, flag in (("_corr", "phi_correction"), ("_smag", "smagorinsky")):
+        if name.endswith(suffix):
+            # the same case with the phi mass correction after every step / the
+            # Smagorinsky relaxation time
+            p, isf, m, phi = make_case(name[: -len(suffix)], storage)
+            setattr(p, flag, 1)
+            return p, isf, m, phi
     rng = np.random.default_rng(sum(map(ord, name)) * 7919)
     if name == "tg_q19":
         p = Params(lx=32, ly=24, lz=16, lattice=19, visc1=0.01, storage=storage)
@@ -123,7 +125,8 @@ def make_case(name: str, storage: str = "f32"):
 
 
 ALL_CASES = ["tg_q19", "q27ho_1c_force", "q27_1c", "q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c",
-             "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr"]
+             "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr", "q27ho_1c_force_smag",
+             "obs_q27ho_2c_dr_smag", "q19_2c_smag"]
 
 
 def run_oracle(name: str, nsteps: int, prec: str = "f64"):

@@ -76,9 +76,13 @@ def test_server_equals_single_box_entry_point(alone, i):
     mg, pg, _ = s.get_fields()
     s.close()
     ms, ps = alone[i]
-    assert np.array_equal(ms, mg, equal_nan=True)
+    # the batched kernel is a separate compilation of the same step: equal
+    # within rounding (alone and in a mix it is the same kernel: equal bits)
+    fl = np.abs(isf) == 1
+    bar = 1e-6 if st == "f32" else 1e-3
+    assert rel_l2(ms, mg, fl) < bar
     if p.twocomponent:
-        assert np.array_equal(ps, pg, equal_nan=True)
+        assert rel_l2(ps, pg, fl) < bar
 
 
 def test_server_fp32_matches_oracle():

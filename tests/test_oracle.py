@@ -115,3 +115,22 @@ def test_phi_mass_correction_restores_the_initial_sum(prec, bar):
     s0 = np.sum(phi)
     assert abs(sums[1] - s0) / s0 < bar
     assert abs(sums[0] - s0) / s0 > 1e-4
+
+
+@pytest.mark.parametrize("name", ["q27ho_1c_force", "obs_q27ho_2c_dr"])
+def test_smagorinsky_changes_the_relaxation(name):
+    """SMAGORINSKI raises tau where the non-equilibrium stress is large
+    (lb_cuda_fused_module.f90:609-616): the run departs from the molecular one
+    by more than the FP64 noise and stays finite."""
+    out = {}
+    for smag in (0, 1):
+        p, isf, m, phi = make_case(name)
+        p.smagorinsky = smag
+        o = O.Oracle(p.oracle_dict(), "f64")
+        o.set_isfluid(isf)
+        o.set_fields(m, phi)
+        o.step(10)
+        out[smag] = o.get_fields()[0]
+    fl = np.abs(isf) == 1
+    assert np.all(np.isfinite(out[1][:, fl]))
+    assert rel_l2(out[1], out[0], fl) > 1e-6
