@@ -45,7 +45,14 @@ template <int TY_> struct Tile {
     static constexpr int R2Y = TY_ + 4, R2N = R2X * R2Y;
     static constexpr int R3Y = TY_ + 6, R3N = R3X * R3Y;
     static constexpr int NRING1 = R1N - NT;  // ring nodes of R1 (84 for 8 rows, 100 for 16)
-    static_assert(R2N <= 2 * NT && R3N <= 3 * NT, "region loops assume at most 2 / 3 nodes per thread");
+    // The ring collisions go to the last RW warps (a warp pays for its slowest
+    // lane, so those warps carry two collisions); the theta work goes to the
+    // other NTH threads only, KTH nodes each, which balances the first phase.
+    static constexpr int RW = (NRING1 + 31) / 32;
+    static constexpr int NTH = NT - 32 * RW;
+    static constexpr int KTH = (R2N + NTH - 1) / NTH;
+    static_assert(R3N <= 3 * NT, "phi loads assume at most 3 nodes per thread");
+    static_assert(KTH <= 3, "theta nodes per thread");
 };
 
 __device__ __forceinline__ int wrap_coord(int g, int n, int periodic, bool& ok) {

@@ -83,7 +83,7 @@ template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int z0,
                                           const int z1) {
     using TL = Tile<TYV>;
-    constexpr int TY = TL::TY, NT = TL::NT, NRING1 = TL::NRING1;
+    constexpr int TY = TL::TY, NT = TL::NT, NRING1 = TL::NRING1, NTH = TL::NTH, KTH = TL::KTH;
     constexpr int R1Y = TL::R1Y, R1N = TL::R1N, R2Y = TL::R2Y, R2N = TL::R2N, R3N = TL::R3N;
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
@@ -116,12 +116,13 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     const R cssq = R(1.0 / 3.0);
 
     // ---- static per-thread node tables (x/y wrap does not change along z) ----
-    // collision nodes: A = tile interior node t; B = ring node for the last NRING1 threads
+    // collision nodes: A = tile interior node t; B = ring node r for the threads
+    // of the last warps (t >= NTH), r = t - NTH < NRING1
     const int nodeA = (ty + 1) * R1X + (tx + 1);
     int nodeB = -1;
     {
-        const int r = t - (NT - NRING1);
-        if (r >= 0) {
+        const int r = t - NTH;
+        if (r >= 0 && r < NRING1) {
             if (r < R1X) nodeB = r;                                        // top row
             else if (r < 2 * R1X) nodeB = (R1Y - 1) * R1X + (r - R1X);     // bottom row
             else if (r < 2 * R1X + TY) nodeB = (r - 2 * R1X + 1) * R1X;    // left column
@@ -156,16 +157,21 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         nby_ok[d] = oky;
     }
 
-    // theta nodes (R2): t and t + NT; phi nodes (R3): t, t + NT, t + 2 NT
-    int r2_off[2] = {0, 0};
-    bool r2_ok[2] = {false, false};
+    // theta nodes (R2): t + k NTH for the first NTH threads; phi nodes (R3): t, t + NT, t + 2 NT
+    int r2_off[KTH];
+    bool r2_ok[KTH];
+#pragma unroll
+    for (int k = 0; k < KTH; ++k) {
+        r2_off[k] = 0;
+        r2_ok[k] = false;
+    }
     int r3_off[3] = {0, 0, 0};
     bool r3_ok[3] = {false, false, false};
     if constexpr (TC) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            int n = t + k * NT;
-            if (n < R2N) {
+        for (int k = 0; k < KTH; ++k) {
+            int n = t + k * NTH;
+            if (t < NTH && n < R2N) {
                 int hx = n % R2X, hy = n / R2X;
                 bool ok = true;
                 int gx = wrap_coord(X0 + hx - 2, nx, p.pbx, ok);
@@ -262,9 +268,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         R* sx = sxys + sxy_slot(q) * R2N;
         R* gg = gxys + gxy_slot(q) * (2 * R2N);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int n = t + k * NT;
-            if (n >= R2N) continue;
+        for (int k = 0; k < KTH; ++k) {
+            const int n = t + k * NTH;
+            if (t >= NTH || n >= R2N) continue;
             const int hx = n % R2X, hy = n / R2X;
             const R* c = f + (hy + 1) * R3X + (hx + 1);
             const R fc = c[0];
@@ -297,9 +303,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         R* th = ths + th_slot(q) * (3 * R2N);
         R* gt = gts + gt_slot(q) * (3 * R1N);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int n = t + k * NT;
-            if (n >= R2N) continue;
+        for (int k = 0; k < KTH; ++k) {
+            const int n = t + k * NTH;
+            if (t >= NTH || n >= R2N) continue;
             const int hx = n % R2X, hy = n / R2X;
             bool fluid = zok && r2_ok[k];
             if (fluid && obs) {
