@@ -259,8 +259,10 @@ def _drain(srv, jobs, nsteps):
 def run_serving(n: int, nsteps: int, seed: int = 7):
     """Solves/s of the batched server against the same solves run one at a
     time on the same engine (max_active = 1: same kernel, same graphs, no
-    batching), the saturated throughput (all submitted at once), and per-solve
-    latency under seeded Poisson arrivals at 1.5x the one-at-a-time rate."""
+    batching) and one at a time through lbf_step (each solve with its own
+    autotuned kernel), the saturated throughput (all submitted at once), and
+    per-solve latency under seeded Poisson arrivals at 1.5x the one-at-a-time
+    rate."""
     import numpy as np
     import lbfast_b200 as lbf
     jobs = serving_jobs(n, seed)
@@ -280,6 +282,16 @@ def run_serving(n: int, nsteps: int, seed: int = 7):
         seq_out = [srv.fetch(i) for i in ids]
     # lattice updates per second of one solve running alone, by box edge
     alone_mlups = {e: e ** 3 * nsteps / float(np.mean(v)) / 1e6 for e, v in sorted(svc.items())}
+    # one at a time through the single-box entry point (lbf_step, autotuned
+    # 16-row kernel), fields uploaded and read back per solve like the server
+    t0 = time.monotonic()
+    for p, m, phi in jobs:
+        s = lbf.Solver(p)
+        s.set_fields(m, phi)
+        s.step(nsteps)
+        s.get_fields(np.float32)
+        s.close()
+    t_step = time.monotonic() - t0
     # batched, saturated
     with lbf.Server(chunk=32) as srv:
         t0 = time.monotonic()
@@ -317,6 +329,7 @@ def run_serving(n: int, nsteps: int, seed: int = 7):
                     "R = edge/4 with a P2 shape perturbation eps ~ U[0.05,0.15], density ratio log-uniform "
                     "[10,1000], D3Q27 two-component DENSRATIO, FP16 storage, nu 0.001, sigma 0.03, width 5, seed 7",
         "solves_per_s": n / t_bat, "solves_per_s_one_at_a_time": n / t_seq, "speedup": t_seq / t_bat,
+        "solves_per_s_lbf_step": n / t_step, "speedup_vs_lbf_step": t_step / t_bat,
         "mlups_batched": lups / t_bat / 1e6, "mlups_one_at_a_time": lups / t_seq / 1e6,
         "mlups_alone_by_edge": alone_mlups,
         "open_loop": {"arrival_rate_per_s": lam, "solves_per_s": n / t_open,

@@ -103,7 +103,9 @@ struct Batch {
     std::vector<int4> h_work;
 };
 
-// tile height of a solve's class: the one requested, else 8 rows
+// tile height of a solve's class: the one requested, else 8 rows.  A batch of
+// small boxes has few 16-row columns to spread over the SMs (measured on the
+// droplet ensemble: 4.9 solves/s with 8 rows, 4.1 with 16).
 int solve_tile(const lbf_params& p) { return p.tile_y ? p.tile_y : 8; }
 
 }  // namespace
