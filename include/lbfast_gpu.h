@@ -230,6 +230,13 @@ int lbf_write_restart_raw(const char* dir, int lx, int ly, int lz, const float* 
 int lbf_read_restart_raw(const char* dir, int lx, int ly, int lz, float* mom10, float* phi, int* iframe,
                          int* iframe2D);
 
+/* VTK ImageData writer of print_vtk_sync (print_module.f90:22-244, 2789-2814):
+ * <dir>/out_rho_NNNNNN.vti, out_vel_... (3 components), and out_press_... when
+ * press is not NULL, byte for byte in the reference's layout (Float32 data;
+ * the reference's PRINTHALF UnsignedShort variant is not provided). */
+int lbf_write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                  const float* press);
+
 /* raw + XDMF writer of print_raw_sync (print_module.f90:2007-2180): writes
  * <dir>/out_rho_NNNNNN.raw/.xdmf, out_vel_..., and out_press_... when press
  * is not NULL. */

@@ -27,7 +27,7 @@ EXPORTED = (
     "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
     "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
     "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning", "lbf_write_restart_raw",
-    "lbf_read_restart_raw",
+    "lbf_read_restart_raw", "lbf_write_vtk",
 )
 SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -94,6 +94,7 @@ def load() -> C.CDLL:
     lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
     lib.lbf_ic_droplet.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
     lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    lib.lbf_write_vtk.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
     lib.lbf_write_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, C.c_int, C.c_int]
     lib.lbf_read_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, P(C.c_int), P(C.c_int)]
     lib.lbf_server_create.argtypes = [P(LbfServerConfig), P(vp)]
@@ -403,6 +404,16 @@ def read_restart_raw(directory: str, lx: int, ly: int, lz: int, twocomponent: bo
     check(load().lbf_read_restart_raw(directory.encode(), lx, ly, lz, _ptr(m, C.c_float), _ptr(p, C.c_float),
                                       C.byref(fr), C.byref(fr2)))
     return m, p, fr.value, fr2.value
+
+
+def write_vtk(directory: str, iframe: int, rho, vel, press=None) -> None:
+    """VTK ImageData files of the reference's print_vtk_sync."""
+    lz, ly, lx = rho.shape
+    r = np.ascontiguousarray(rho, dtype=np.float32)
+    v = np.ascontiguousarray(np.moveaxis(vel, 0, -1), dtype=np.float32)
+    p = None if press is None else np.ascontiguousarray(press, dtype=np.float32)
+    check(load().lbf_write_vtk(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float), _ptr(v, C.c_float),
+                               _ptr(p, C.c_float)))
 
 
 def write_raw_xdmf(directory: str, iframe: int, rho, vel, press=None) -> None:

@@ -432,6 +432,65 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
     return LBF_OK;
 }
 
+// ---- VTK ImageData (print_module.f90:22-244 header_vtk / footer_vtk, 2789-2814) ----
+// One .vti file per variable: a fixed-width XML header whose last byte is the
+// '_' that opens the appended raw data, the data byte count as int32, the
+// float32 values (vectors interleaved per node), and a 30-byte footer.
+namespace {
+std::string rjust(long long v, int w) {
+    std::string s = std::to_string(v);
+    return s.size() >= (size_t)w ? s : std::string(w - s.size(), ' ') + s;
+}
+
+int write_vti(const std::string& path, const char* name8, int ncomp, int lx, int ly, int lz, const float* data) {
+    const long long N = (long long)lx * ly * lz;
+    const std::string ext = rjust(1, 6) + " " + rjust(lx, 6) + " " + rjust(1, 6) + " " + rjust(ly, 6) + " " +
+                            rjust(1, 6) + " " + rjust(lz, 6);
+    // the reference assigns each line to a fixed-width field (padding with blanks)
+    auto field = [](std::string s, size_t w) {
+        s.resize(w - 1, ' ');
+        return s + '\n';
+    };
+    std::string h;
+    h += field("<?xml version=\"1.0\"?>", 22);
+    h += field("<VTKFile type=\"ImageData\" version=\"0.1\" byte_order=\"LittleEndian\">", 67);
+    h += field("  <ImageData WholeExtent=\"" + ext + "\">", 70);
+    h += field("    <Piece Extent=\"" + ext + "\">", 63);
+    h += field("      <PointData>", 18);
+    h += field(std::string("        <DataArray type=\"Float32\" Name=\"") + name8 + "\" NumberOfComponents=\"" +
+                   std::to_string(ncomp) + "\" format=\"appended\" offset=\"" + rjust(0, 12) + "\"/>",
+               115);
+    h += field("      </PointData>", 19);
+    h += field("    </Piece>", 13);
+    h += field("  </ImageData>", 15);
+    h += field("  <AppendedData encoding=\"raw\">", 32);
+    h += "_";
+    const std::string foot = std::string("\n") + "  </AppendedData>\n" + "</VTKFile>\n";
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return LBF_E_IO;
+    const int32_t nbytes = (int32_t)(ncomp * N * (long long)sizeof(float));
+    bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+    ok = ok && std::fwrite(&nbytes, sizeof nbytes, 1, f) == 1;
+    ok = ok && std::fwrite(data, sizeof(float), ncomp * N, f) == (size_t)(ncomp * N);
+    ok = ok && std::fwrite(foot.data(), 1, foot.size(), f) == foot.size();
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? LBF_OK : LBF_E_IO;
+}
+}  // namespace
+
+int lbf_write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                  const float* press) {
+    if (!dir || !rho || !vel || lx < 1 || ly < 1 || lz < 1) return LBF_E_ARG;
+    char num[16];
+    std::snprintf(num, sizeof(num), "%06d", iframe < 0 ? 0 : (iframe > 999999 ? 999999 : iframe));
+    std::string d = dir;
+    if (!d.empty() && d.back() != '/') d += '/';
+    int rc = write_vti(d + "out_rho_" + num + ".vti", "rho     ", 1, lx, ly, lz, rho);
+    if (rc == LBF_OK) rc = write_vti(d + "out_vel_" + num + ".vti", "vel     ", 3, lx, ly, lz, vel);
+    if (rc == LBF_OK && press) rc = write_vti(d + "out_press_" + num + ".vti", "press   ", 1, lx, ly, lz, press);
+    return rc;
+}
+
 // ---- restart.raw (print_module.f90:1030-1474 and 1474-1677) ----
 // The reference's restart is one time level in float32, stream-unformatted:
 // the ten moment fields in the order of its hfields indices 1,2,3,4,5,8,9,6,10,7

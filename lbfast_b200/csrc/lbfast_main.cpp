@@ -194,14 +194,17 @@ int main(int argc, char** argv) {
     // ---- output set-up: print_module.f90:277-445 ----
     std::vector<float> rho(N), vel(3 * N), press(N);
     const bool do_raw = run.lprint && run.lraw;
-    if (do_raw || run.lwriterestart) mkdir("output", 0755);
-    if (run.lvtk) std::fprintf(stderr, "lbfast: lvtk ignored (VTK output is not provided)\n");
+    const bool do_vtk = run.lprint && run.lvtk;
+    if (do_raw || do_vtk || run.lwriterestart) mkdir("output", 0755);
     if (run.nplanes > 0) std::fprintf(stderr, "lbfast: nplanes ignored (2-D plane output is not provided)\n");
     if (run.lprint && !run.lrestart) {
         CHECK(lbf_get_print_fields(h, rho.data(), vel.data(), press.data()));
         if (do_raw)
             CHECK(lbf_write_raw_xdmf("output", iframe, lx, ly, lz, rho.data(), vel.data(),
                                      fl.writepress && p.twocomponent ? press.data() : nullptr));
+        if (do_vtk)
+            CHECK(lbf_write_vtk("output", iframe, lx, ly, lz, rho.data(), vel.data(),
+                                fl.writepress && p.twocomponent ? press.data() : nullptr));
     }
 
     // ---- time loop: integrator_module.f90:266-827 (steps come in FLIP/FLOP pairs) ----
@@ -219,6 +222,9 @@ int main(int argc, char** argv) {
                 if (do_raw)
                     CHECK(lbf_write_raw_xdmf("output", iframe, lx, ly, lz, rho.data(), vel.data(),
                                              fl.writepress && p.twocomponent ? press.data() : nullptr));
+                if (do_vtk)
+                    CHECK(lbf_write_vtk("output", iframe, lx, ly, lz, rho.data(), vel.data(),
+                                        fl.writepress && p.twocomponent ? press.data() : nullptr));
             }
             if (at_term) {
                 int i = run.iprobe - 1, j = run.jprobe - 1, k = run.kprobe - 1;

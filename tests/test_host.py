@@ -173,3 +173,32 @@ def test_restart_file_layout_and_round_trip(tmp_path, two):
         assert np.array_equal(p2, phi)
     with pytest.raises(L.LbfError):  # size check: a one-component file is not a two-component restart
         L.read_restart_raw(str(tmp_path), lx, ly, lz, not two)
+
+
+def test_vtk_files_in_the_reference_layout(tmp_path):
+    """print_vtk_sync (print_module.f90:22-244, 2789-2814): fixed-width XML
+    header of 435 bytes ending in '_', int32 byte count, float32 data (vectors
+    interleaved per node), 30-byte footer; names out_<var>_NNNNNN.vti."""
+    lx, ly, lz = 36, 20, 7
+    rng = np.random.default_rng(5)
+    rho = rng.random((lz, ly, lx)).astype(np.float32)
+    vel = rng.standard_normal((3, lz, ly, lx)).astype(np.float32)
+    L.write_vtk(str(tmp_path), 12, rho, vel)
+    ext = "     1     36      1     20      1      7"
+    for var, data, nc in (("rho", rho, 1), ("vel", np.moveaxis(vel, 0, -1), 3)):
+        b = (tmp_path / f"out_{var}_000012.vti").read_bytes()
+        lines = ['<?xml version="1.0"?>',
+                 '<VTKFile type="ImageData" version="0.1" byte_order="LittleEndian">',
+                 f'  <ImageData WholeExtent="{ext}">', f'    <Piece Extent="{ext}">', "      <PointData>",
+                 f'        <DataArray type="Float32" Name="{var:<8s}" NumberOfComponents="{nc}" '
+                 f'format="appended" offset="{0:>12d}"/>',
+                 "      </PointData>", "    </Piece>", "  </ImageData>", '  <AppendedData encoding="raw">']
+        widths = [22, 67, 70, 63, 18, 115, 19, 13, 15, 32]
+        head = "".join(s.ljust(w - 1) + "\n" for s, w in zip(lines, widths)) + "_"
+        assert len(head) == 435
+        assert b[:435] == head.encode()
+        n = lx * ly * lz * nc * 4
+        assert np.frombuffer(b[435:439], np.int32)[0] == n
+        assert np.array_equal(np.frombuffer(b[439:439 + n], np.float32), data.reshape(-1))
+        assert b[439 + n:] == b"\n  </AppendedData>\n</VTKFile>\n"
+    assert not (tmp_path / "out_press_000012.vti").exists()
