@@ -47,6 +47,8 @@ int fail(int code, const char* fmt, ...) {
 const int EXh[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, -1, 1, 1, -1};
 const int EYh[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, -1, 1};
 const int EZh[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1};
+// is D3Q27 link l a link of the lattice: D3Q19 = links 0-18, D3Q15 = links 0-6 and 19-26
+bool link_in(int lat, int l) { return lat == 27 || (lat == 19 ? l < 19 : (l < 7 || l >= 19)); }
 
 }  // namespace
 
@@ -289,7 +291,8 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (p->lx < 1 || p->ly < 1 || p->lz < 1) return fail(LBF_E_ARG, "box must be at least 1^3");
     if ((long long)p->lx * p->ly * p->lz > (1LL << 31) - 1)
         return fail(LBF_E_ARG, "box of %lld nodes exceeds 2^31-1", (long long)p->lx * p->ly * p->lz);
-    if (p->lattice != 19 && p->lattice != 27) return fail(LBF_E_UNSUPPORTED, "LATTICE %d not supported (19 or 27)", p->lattice);
+    if (p->lattice != 15 && p->lattice != 19 && p->lattice != 27)
+        return fail(LBF_E_UNSUPPORTED, "LATTICE %d not supported (15, 19 or 27)", p->lattice);
     if (p->highorder && p->lattice != 27) return fail(LBF_E_ARG, "HIGHORDER requires LATTICE 27");
     if (p->densratio && !p->twocomponent) return fail(LBF_E_ARG, "DENSRATIO requires TWOCOMPONENT");
     if (p->storage < 0 || p->storage > 3) return fail(LBF_E_ARG, "unknown storage %d", p->storage);
@@ -396,7 +399,7 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
     // in double; they depend on isfluid only.
     const int pb[3] = {h->p.pbc_x, h->p.pbc_y, h->p.pbc_z};
     const int dims[3] = {nx, ny, nz};
-    const int nl = h->p.lattice == 27 ? 27 : 19;
+    const int lat = h->p.lattice;
     auto isf_at = [&](int x, int y, int z) -> int {
         int c[3] = {x, y, z};
         for (int d = 0; d < 3; ++d) {
@@ -416,7 +419,8 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
                 long long c = ((long long)k * ny + j) * nx + i;
                 if (isf[c] != 0) continue;
                 double wx = 0, wy = 0, wz = 0;
-                for (int l = 1; l < nl; ++l) {
+                for (int l = 1; l < 27; ++l) {
+                    if (!link_in(lat, l)) continue;
                     int d2 = EXh[l] * EXh[l] + EYh[l] * EYh[l] + EZh[l] * EZh[l];
                     if (isf_at(i + EXh[l], j + EYh[l], k + EZh[l]) == 0) continue;
                     double sc = d2 == 1 ? 1.0 : d2 == 2 ? 0.5 : 1.0 / 3.0;
@@ -429,7 +433,8 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
                 wx /= wn; wy /= wn; wz /= wn;
                 double best = -1.0e30;
                 int bl = -1;
-                for (int l = 1; l < nl; ++l) {
+                for (int l = 1; l < 27; ++l) {
+                    if (!link_in(lat, l)) continue;
                     int d2 = EXh[l] * EXh[l] + EYh[l] * EYh[l] + EZh[l] * EZh[l];
                     int f = isf_at(i + EXh[l], j + EYh[l], k + EZh[l]);
                     if (f != 1 && f != -1) continue;

@@ -23,6 +23,10 @@ const int EZh[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -
 
 inline long long lin(int i, int j, int k, int lx, int ly) { return ((long long)k * ly + j) * lx + i; }
 
+// is D3Q27 link l a link of the lattice: D3Q19 = links 0-18 (vars_module.f90:666-684),
+// D3Q15 = links 0-6 and 19-26 (vars_module.f90:685-703), in the reference's order
+inline bool link_in(int lat, int l) { return lat == 27 || (lat == 19 ? l < 19 : (l < 7 || l >= 19)); }
+
 // Fortran NINT: round half away from zero
 inline double nint_f(double a) { return a >= 0 ? std::floor(a + 0.5) : -std::floor(-a + 0.5); }
 }  // namespace
@@ -33,7 +37,7 @@ extern "C" {
 int lbf_mark_isfluid(int lx, int ly, int lz, int pbc_x, int pbc_y, int pbc_z, int lattice, int obstacles,
                      const int8_t* raw, int8_t* out) {
     if (lx < 1 || ly < 1 || lz < 1 || !out) return LBF_E_ARG;
-    if (lattice != 19 && lattice != 27) return LBF_E_UNSUPPORTED;
+    if (lattice != 15 && lattice != 19 && lattice != 27) return LBF_E_UNSUPPORTED;
     const long long N = (long long)lx * ly * lz;
     std::vector<int8_t> isf(N);
     for (long long c = 0; c < N; ++c) isf[c] = raw ? (raw[c] != 0 ? 1 : 0) : 1;
@@ -48,14 +52,14 @@ int lbf_mark_isfluid(int lx, int ly, int lz, int pbc_x, int pbc_y, int pbc_z, in
     }
     const int dims[3] = {lx, ly, lz};
     const int pb[3] = {pbc_x, pbc_y, pbc_z};
-    const int nl = lattice == 27 ? 27 : 19;
     for (long long c = 0; c < N; ++c) out[c] = isf[c];
     for (int k = 0; k < lz; ++k)
         for (int j = 0; j < ly; ++j)
             for (int i = 0; i < lx; ++i) {
                 long long c = lin(i, j, k, lx, ly);
                 if (isf[c] != 1) continue;
-                for (int l = 1; l < nl; ++l) {
+                for (int l = 1; l < 27; ++l) {
+                    if (!link_in(lattice, l)) continue;
                     int q[3] = {i + EXh[l], j + EYh[l], k + EZh[l]};
                     int v = 1;  // halo in a non-periodic direction keeps isfluid = 1
                     bool inside = true;
@@ -75,14 +79,14 @@ int lbf_mark_isfluid(int lx, int ly, int lz, int pbc_x, int pbc_y, int pbc_z, in
 // init_conditions_module.f90:492-541
 int lbf_seed_solid_phi(int lx, int ly, int lz, int lattice, const int8_t* isfluid, double* phi) {
     if (!isfluid || !phi) return LBF_E_ARG;
-    const int nl = lattice == 27 ? 27 : 19;
     for (int k = 0; k < lz; ++k)
         for (int j = 0; j < ly; ++j)
             for (int i = 0; i < lx; ++i) {
                 long long c = lin(i, j, k, lx, ly);
                 if (isfluid[c] != 0) continue;
                 double num = 0, den = 0;
-                for (int l = 1; l < nl; ++l) {
+                for (int l = 1; l < 27; ++l) {
+                    if (!link_in(lattice, l)) continue;
                     int ni = i + EXh[l], nj = j + EYh[l], nk = k + EZh[l];
                     if (ni < 0 || ni >= lx || nj < 0 || nj >= ly || nk < 0 || nk >= lz) continue;
                     long long n = lin(ni, nj, nk, lx, ly);

@@ -107,6 +107,7 @@ template <typename S, typename R> void fill_params(const StepArgs& a, void* dst)
 
 // the five kernel classes of one storage type and tile height
 template <typename S, typename R, int TYV> StepLauncher step_table(int lat, int ho, int tc) {
+    if (lat == 15 && !ho) return tc ? &launch_stream<15, false, true, S, R, TYV> : &launch_stream<15, false, false, S, R, TYV>;
     if (lat == 19 && !ho) return tc ? &launch_stream<19, false, true, S, R, TYV> : &launch_stream<19, false, false, S, R, TYV>;
     if (lat == 27 && ho) return tc ? &launch_stream<27, true, true, S, R, TYV> : &launch_stream<27, true, false, S, R, TYV>;
     if (lat == 27 && !ho) return tc ? &launch_stream<27, false, true, S, R, TYV> : &launch_stream<27, false, false, S, R, TYV>;
@@ -120,6 +121,10 @@ template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho,
     o.tile_y = TYV;
     o.launch = nullptr;
     o.resident = nullptr;
+    if (lat == 15 && !ho) {
+        o.launch = tc ? &launch_stream_batched<15, false, true, S, R, TYV> : &launch_stream_batched<15, false, false, S, R, TYV>;
+        o.resident = tc ? &batched_resident<15, false, true, S, R, TYV> : &batched_resident<15, false, false, S, R, TYV>;
+    }
     if (lat == 19 && !ho) {
         o.launch = tc ? &launch_stream_batched<19, false, true, S, R, TYV> : &launch_stream_batched<19, false, false, S, R, TYV>;
         o.resident = tc ? &batched_resident<19, false, true, S, R, TYV> : &batched_resident<19, false, false, S, R, TYV>;

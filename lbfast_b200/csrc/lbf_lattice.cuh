@@ -26,7 +26,10 @@
 
 namespace lbf {
 
-// D3Q27 link table (D3Q19 = first 19 entries)
+// D3Q27 link table.  D3Q19 is its first 19 entries (vars_module.f90:666-684),
+// D3Q15 the entries 0-6 and 19-26 (vars_module.f90:685-703): both in the
+// reference's own link order, so loops over the D3Q27 indices of a lattice's
+// links visit them in the reference's order.
 __host__ __device__ constexpr int EX(int l) {
     constexpr int t[27] = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1,-1, 1, 1,-1};
     return t[l];
@@ -43,13 +46,23 @@ __host__ __device__ constexpr int OPP(int l) {
     constexpr int t[27] = {0, 2, 1, 4, 3, 6, 5, 8, 7,10, 9,12,11,14,13,16,15,18,17,20,19,22,21,24,23,26,25};
     return t[l];
 }
-// weight of link l; D3Q27: 8/27, 2/27, 1/54, 1/216; D3Q19: 1/3, 1/18, 1/36
+// is D3Q27 link l a link of lattice LAT (27, 19 or 15)
+template <int LAT> __host__ __device__ constexpr bool IN(int l) {
+    return LAT == 27 ? true : LAT == 19 ? l < 19 : (l < 7 || l >= 19);
+}
+__host__ __device__ constexpr bool in_lattice(int lat, int l) {
+    return lat == 27 ? true : lat == 19 ? l < 19 : (l < 7 || l >= 19);
+}
+// weight of link l; D3Q27: 8/27, 2/27, 1/54, 1/216; D3Q19: 1/3, 1/18, 1/36;
+// D3Q15: 2/9, 1/9, 1/72
 template <int LAT> __host__ __device__ constexpr double WL(int l) {
     return LAT == 27 ? ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 8.0 / 27.0 :
                         (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 2.0 / 27.0 :
                         (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 2 ? 1.0 / 54.0 : 1.0 / 216.0)
-                     : ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 1.0 / 3.0 :
-                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 1.0 / 18.0 : 1.0 / 36.0);
+         : LAT == 19 ? ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 1.0 / 3.0 :
+                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 1.0 / 18.0 : 1.0 / 36.0)
+                     : ((EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 0 ? 2.0 / 9.0 :
+                        (EX(l) * EX(l) + EY(l) * EY(l) + EZ(l) * EZ(l)) == 1 ? 1.0 / 9.0 : 1.0 / 72.0);
 }
 // link index of velocity (cx,cy,cz) in the D3Q27 ordering
 __host__ __device__ constexpr int LINK(int cx, int cy, int cz) {

@@ -644,38 +644,40 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                             fpop[LINK(a - 1, b - 1, 1)] = vp;
                         }
                 } else {
+                    // D3Q19 / D3Q15: the second-order expansion link by link (D3Q27 indices)
                     const R base = m0 - R(1.5) * (mxx + myy + mzz);
 #pragma unroll
-                    for (int l = 0; l < 19; ++l) {
+                    for (int l = 0; l < 27; ++l) {
+                        if (!IN<LAT>(l)) continue;
                         const int cx = EX(l), cy = EY(l), cz = EZ(l);
                         R s = base;
                         s += R(3) * (R(cx) * mx + R(cy) * my + R(cz) * mz);
                         s += R(4.5) * (R(cx * cx) * mxx + R(cy * cy) * myy + R(cz * cz) * mzz);
                         s += R(9) * (R(cx * cy) * mxy + R(cx * cz) * mxz + R(cy * cz) * myz);
-                        fpop[l] = R(WL<19>(l)) * s;
+                        fpop[l] = R(WL<LAT>(l)) * s;
                     }
                 }
             } else {
 #pragma unroll
-                for (int l = 0; l < LAT; ++l) fpop[l] = R(0);
+                for (int l = 0; l < 27; ++l) fpop[l] = R(0);
             }
 #pragma unroll
             for (int g = 0; g < 9; ++g) {
                 const int cx = g % 3 - 1, cy = g / 3 - 1;
-                constexpr bool q19 = LAT == 19;
-                const bool has_z = !q19 || (cx * cx + cy * cy) < 2;  // D3Q19 has no (+-1, +-1, +-1)
+                // links the lattice lacks carry 0 (D3Q19: no corners, D3Q15: no edges)
                 R2 v;
-                v.x = has_z ? fpop[LINK(cx, cy, -1)] : R(0);
-                v.y = fpop[LINK(cx, cy, 0)];
+                v.x = IN<LAT>(LINK(cx, cy, -1)) ? fpop[LINK(cx, cy, -1)] : R(0);
+                v.y = IN<LAT>(LINK(cx, cy, 0)) ? fpop[LINK(cx, cy, 0)] : R(0);
                 pops2[g * R1N + node] = v;
-                pops1[g * R1N + node] = has_z ? fpop[LINK(cx, cy, 1)] : R(0);
+                pops1[g * R1N + node] = IN<LAT>(LINK(cx, cy, 1)) ? fpop[LINK(cx, cy, 1)] : R(0);
             }
 
             // ---- obstacle bounce-back: lb_cuda_boundary_module.f90:162-199 ----
             if (interior && obs && isf == -1) {
                 const R om1 = R(1) - som;
 #pragma unroll
-                for (int l = 1; l < LAT; ++l) {
+                for (int l = 1; l < 27; ++l) {
+                    if (!IN<LAT>(l)) continue;
                     const int cx = EX(l), cy = EY(l), cz = EZ(l);
                     const int ix = 1 - cx, iy = 1 - cy;
                     bool zk = true;

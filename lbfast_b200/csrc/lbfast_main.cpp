@@ -1,7 +1,7 @@
 // lbfast_main.cpp -- driver program in the shape of LBFAST.f90 on top of the
 // C ABI (include/lbfast_gpu.h).
 //
-//   lbfast [-DLATTICE=19|27] [-DHIGHORDER] [-DTWOCOMPONENT] [-DDENSRATIO]
+//   lbfast [-DLATTICE=15|19|27] [-DHIGHORDER] [-DTWOCOMPONENT] [-DDENSRATIO]
 //          [-DINTERNAL_OBSTACLES] [-DWETTABILITY] [-DPRINTPHI] [-DWRITEPRESS] [-DSMAGORINSKI]
 //          [-DTAYLORGREEN|-DLAPLACE|-DLAMBTEST] [--storage=f32|f16|bf16|f64]
 //          input.inp
@@ -66,6 +66,7 @@ Flags parse_flags(int argc, char** argv) {
         std::string a = argv[i];
         if (a == "-DLATTICE=27") fl.lattice = 27;
         else if (a == "-DLATTICE=19") fl.lattice = 19;
+        else if (a == "-DLATTICE=15") fl.lattice = 15;
         else if (a == "-DHIGHORDER") fl.highorder = true;
         else if (a == "-DTWOCOMPONENT") fl.twocomponent = true;
         else if (a == "-DDENSRATIO") fl.densratio = true;

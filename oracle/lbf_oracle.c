@@ -27,7 +27,7 @@
  *   update_phi            lb_cuda_update_phi_module.f90:19-104
  *   obstacle bounce-back  lb_cuda_boundary_module.f90:19-216
  *   copy_print            print_module.f90:638-776
- *   lattice tables        vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19)
+ *   lattice tables        vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15)
  *   parameter derivation  LBFAST.f90:212-219
  *
  * The fields live on a padded grid with one halo layer (the reference's
@@ -67,7 +67,7 @@ typedef REAL real;
 typedef struct orc_params {
     int lx, ly, lz;
     int pbc_x, pbc_y, pbc_z;
-    int lattice;     /* 19 or 27 */
+    int lattice;     /* 15, 19 or 27 */
     int highorder;   /* HIGHORDER (LATTICE 27 only) */
     int twocomp;     /* TWOCOMPONENT */
     int densratio;   /* DENSRATIO (implies INTERFACE_INCOMP) */
@@ -79,7 +79,7 @@ typedef struct orc_params {
     int smagorinsky;    /* SMAGORINSKI LES relaxation time (see smag_omega) */
 } orc_params;
 
-/* ---- lattice tables: vars_module.f90:319-338 (D3Q27) and 666-684 (D3Q19) ---- */
+/* ---- lattice tables: vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15) ---- */
 static const int ex27[27] = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1,-1, 1, 1,-1};
 static const int ey27[27] = {0, 0, 0, 1,-1, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1,-1, 1,-1, 1};
 static const int ez27[27] = {0, 0, 0, 0, 0, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 1,-1, 1,-1, 1,-1, 1,-1, 1,-1,-1, 1};
@@ -89,7 +89,7 @@ typedef struct orc_state {
     orc_params p;
     int nx, ny, nz, NX, NY, NZ;
     long npad;
-    int nl;                    /* links incl. rest: 19 or 27 */
+    int nl;                    /* links incl. rest: 15, 19 or 27 */
     int ex[27], ey[27], ez[27], opp[27];
     real w[27];
     real minv[27][27];         /* minv[r][l] = Minv_mrt(r,l) */
@@ -139,13 +139,26 @@ static void build_tables(orc_state *s)
             int n2 = ex27[l] * ex27[l] + ey27[l] * ey27[l] + ez27[l] * ez27[l];
             s->w[l] = (real)(n2 == 0 ? 8.0 / 27.0 : n2 == 1 ? 2.0 / 27.0 : n2 == 2 ? 1.0 / 54.0 : 1.0 / 216.0);
         }
-    } else {
+    } else if (s->p.lattice == 19) {
         /* D3Q19 is the first 19 links of the D3Q27 ordering (vars_module.f90:670-680) */
         s->nl = 19;
         for (l = 0; l < 19; l++) {
             s->ex[l] = ex27[l]; s->ey[l] = ey27[l]; s->ez[l] = ez27[l]; s->opp[l] = opp27[l];
             int n2 = ex27[l] * ex27[l] + ey27[l] * ey27[l] + ez27[l] * ez27[l];
             s->w[l] = (real)(n2 == 0 ? 1.0 / 3.0 : n2 == 1 ? 1.0 / 18.0 : 1.0 / 36.0);
+        }
+    } else {
+        /* D3Q15 (vars_module.f90:685-703): rest, faces and corners, in the
+         * reference's order, which is the D3Q27 order of those links; opposite
+         * pairs stay adjacent (opp = 0,2,1,4,3,...) */
+        static const int l15[15] = {0, 1, 2, 3, 4, 5, 6, 19, 20, 21, 22, 23, 24, 25, 26};
+        s->nl = 15;
+        for (l = 0; l < 15; l++) {
+            int m = l15[l];
+            s->ex[l] = ex27[m]; s->ey[l] = ey27[m]; s->ez[l] = ez27[m];
+            s->opp[l] = l == 0 ? 0 : (l % 2 ? l + 1 : l - 1);
+            int n2 = ex27[m] * ex27[m] + ey27[m] * ey27[m] + ez27[m] * ez27[m];
+            s->w[l] = (real)(n2 == 0 ? 2.0 / 9.0 : n2 == 1 ? 1.0 / 9.0 : 1.0 / 72.0);
         }
     }
     /* Minv_mrt(r,l) = w_l H_r(c_l) / <H_r,H_r>_w  (vars_module.f90:360-521, checked

@@ -163,6 +163,16 @@ EY27 = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0, 1
 EZ27 = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1])
 
 
+def lattice_links(lattice: int):
+    """D3Q27 indices of the links of a lattice, in the reference's order:
+    D3Q19 = 0-18 (vars_module.f90:666-684), D3Q15 = 0-6 and 19-26 (:685-703)."""
+    if lattice == 27:
+        return list(range(27))
+    if lattice == 19:
+        return list(range(19))
+    return list(range(7)) + list(range(19, 27))
+
+
 def mark_isfluid(solid: np.ndarray, pbc, lattice: int, obstacles: bool) -> np.ndarray:
     """LBFAST.f90:258-325.  ``solid`` (lz, ly, lx) bool marks nodes read from
     isfluid.raw as 0; returns int8 isfluid in {1, -1, 0}.  The halo is 1 in
@@ -191,10 +201,9 @@ def mark_isfluid(solid: np.ndarray, pbc, lattice: int, obstacles: bool) -> np.nd
     if pbc[2]:
         pad[0, :, :] = pad[lz, :, :]
         pad[lz + 1, :, :] = pad[1, :, :]
-    nl = 27 if lattice == 27 else 19
     out = isf.copy()
     core = pad[1:-1, 1:-1, 1:-1]
-    for l in range(1, nl):
+    for l in lattice_links(lattice)[1:]:
         nb = pad[1 + EZ27[l]:1 + EZ27[l] + lz, 1 + EY27[l]:1 + EY27[l] + ly, 1 + EX27[l]:1 + EX27[l] + lx]
         out[(core == 1) & (np.abs(nb) != 1)] = -1
     return out
@@ -254,7 +263,6 @@ def seed_solid_phi(phi: np.ndarray, isf: np.ndarray, lattice: int = 27) -> np.nd
     no fluid neighbour gets 0/0, i.e. NaN, exactly as the reference."""
     lz, ly, lx = phi.shape
     out = phi.copy()
-    nl = 27 if lattice == 27 else 19
     num = np.zeros_like(phi)
     den = np.zeros_like(phi)
     pad_phi = np.zeros((lz + 2, ly + 2, lx + 2))
@@ -263,7 +271,7 @@ def seed_solid_phi(phi: np.ndarray, isf: np.ndarray, lattice: int = 27) -> np.nd
     pad_isf[1:-1, 1:-1, 1:-1] = isf
     inside = np.zeros((lz + 2, ly + 2, lx + 2), dtype=bool)
     inside[1:-1, 1:-1, 1:-1] = True
-    for l in range(1, nl):
+    for l in lattice_links(lattice)[1:]:
         d2 = EX27[l] ** 2 + EY27[l] ** 2 + EZ27[l] ** 2
         sc = 1.0 if d2 == 1 else (0.70710678118654752440 if d2 == 2 else 0.57735026918962576450)
         sl = (slice(1 + EZ27[l], 1 + EZ27[l] + lz), slice(1 + EY27[l], 1 + EY27[l] + ly),

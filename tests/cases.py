@@ -72,11 +72,12 @@ def make_case(name: str, storage: str = "f32"):
         p = Params(lx=24, ly=16, lz=20, lattice=27, highorder=1, visc1=0.05, fx=1e-5, fy=-2e-5, fz=5e-6,
                    storage=storage)
         return p, np.ones(p.shape, np.int8), _random_moments(rng, p.shape), None
-    if name == "q27_1c":
-        p = Params(lx=20, ly=12, lz=10, lattice=27, highorder=0, visc1=0.03, fx=2e-5, storage=storage)
+    if name in ("q27_1c", "q15_1c"):
+        p = Params(lx=20, ly=12, lz=10, lattice=27 if name == "q27_1c" else 15, highorder=0, visc1=0.03, fx=2e-5,
+                   storage=storage)
         return p, np.ones(p.shape, np.int8), _random_moments(rng, p.shape), None
-    if name in ("q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c"):
-        lat = 19 if name.startswith("q19") else 27
+    if name in ("q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c", "q15_2c_dr"):
+        lat = int(name[1:3])
         ho = 1 if "ho" in name else 0
         dr = 1 if name.endswith("dr") else 0
         L = (40, 24, 28)
@@ -86,8 +87,8 @@ def make_case(name: str, storage: str = "f32"):
         m, phi = O.ic_droplet(L[0], L[1], L[2], (20.5, 12.0, 14.5), 7.0, 3.0, 0.03, p.rho_r, p.rho_b, bool(dr))
         m = m + _random_moments(rng, p.shape, amp_u=0.005, amp_p=0.001, amp_neq=1e-5)
         return p, np.ones(p.shape, np.int8), m, phi
-    if name in ("obs_q27ho_2c_dr", "obs_q19_2c_dr"):
-        lat = 19 if "q19" in name else 27
+    if name in ("obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q15_2c_dr"):
+        lat = 19 if "q19" in name else (15 if "q15" in name else 27)
         ho = 1 if "ho" in name else 0
         L = (36, 20, 24)
         p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_y=0, lattice=lat, highorder=ho, twocomponent=1, densratio=1,
@@ -96,7 +97,7 @@ def make_case(name: str, storage: str = "f32"):
         if lat == 27:
             solid = _spheres_solid(rng, p.shape, 4, 2.5, 4.5)
         else:
-            # D3Q19 seeds solid phi from 18 neighbours but the phi gradient reads 26:
+            # D3Q19 / D3Q15 seed solid phi from 18 / 14 neighbours but the phi gradient reads 26:
             # a sphere's staircase leaves solid nodes that touch fluid only across a
             # cube corner, whose seed is 0/0 (NaN in the reference too).  A cuboid
             # has no such nodes.
@@ -126,7 +127,7 @@ def make_case(name: str, storage: str = "f32"):
 
 ALL_CASES = ["tg_q19", "q27ho_1c_force", "q27_1c", "q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c",
              "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr", "q27ho_1c_force_smag",
-             "obs_q27ho_2c_dr_smag", "q19_2c_smag"]
+             "obs_q27ho_2c_dr_smag", "q19_2c_smag", "q15_1c", "q15_2c_dr", "obs_q15_2c_dr"]
 
 
 def run_oracle(name: str, nsteps: int, prec: str = "f64"):

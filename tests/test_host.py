@@ -133,7 +133,7 @@ def test_raw_xdmf_writer(tmp_path):
     assert 'Dimensions="3 4 5"' in x and 'Dimensions="3 4 5 3"' in x and "out_vel_000007.raw" in x
 
 
-@pytest.mark.parametrize("bad", [dict(lattice=15), dict(highorder=1, lattice=19), dict(densratio=1),
+@pytest.mark.parametrize("bad", [dict(lattice=13), dict(highorder=1, lattice=19), dict(densratio=1),
                                  dict(lx=0), dict(storage="f8"), dict(visc1=-1.0)])
 def test_create_rejects_invalid_parameters_before_device_work(bad):
     kw = dict(lx=8, ly=8, lz=8, lattice=27)
