@@ -250,7 +250,7 @@ int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, cons
  * budget (first in, first out), its fields stay in device memory until it
  * finishes, and every time step of all resident solves of one kernel class
  * (lattice, HIGHORDER, TWOCOMPONENT, storage) is ONE kernel launch over a
- * work list of (solve, tile, z segment) items, replayed as a captured CUDA
+ * work list of (solve, tile column, z range) items, replayed as a captured CUDA
  * graph of `chunk` steps.  Solves that arrive while others run are admitted
  * at the next chunk boundary.  A solve's result does not depend on what else
  * is resident.  Each call must come from one host thread at a time.

@@ -42,7 +42,7 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     static bool attr_set = false;
-    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
+    const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -70,11 +70,12 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
 }
 
 // One launch advancing many boxes of one kernel class: d_boxes holds one
-// StepParams per box, d_work one (box, tile x, tile y, z segment) per CTA.
+// StepParams per box, d_work one (box, first column-plane, end column-plane)
+// per CTA.
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
 cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st) {
     static bool attr_set = false;
-    const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
+    const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -90,7 +91,7 @@ cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int n
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV> int batched_resident() {
     static int resident = 0;
     if (!resident) {
-        const size_t smem = stream_smem_bytes_v2<LAT, TC, S, R, TYV>();
+        const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
         if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV>,

@@ -7,7 +7,7 @@
 // mostly idle.  Here every resident solve keeps its fields in device memory
 // and one launch of the batched step kernel advances ALL resident solves of a
 // kernel class by one time step: the launch walks a work list of (solve,
-// tile x, tile y, z segment) items, one per CTA, whose per-solve parameters
+// range of column-planes) items, one per CTA, whose per-solve parameters
 // (pointers of the current and next time level, scales, physics) sit in a
 // device array.  A chunk of steps is captured once as a CUDA graph and
 // replayed until the set of resident solves changes.

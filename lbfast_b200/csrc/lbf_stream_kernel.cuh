@@ -68,7 +68,7 @@ template <typename R> struct Vec2;
 template <> struct Vec2<float> { using type = float2; };
 template <> struct Vec2<double> { using type = double2; };
 
-template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes_v2() {
+template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes() {
     constexpr int R1N = Tile<TYV>::R1N, R2N = Tile<TYV>::R2N, R3N = Tile<TYV>::R3N;
     size_t b = sizeof(R) * size_t(27) * R1N;  // populations: 9 (cx, cy) groups x 3 cz
     if (TC)
