@@ -68,7 +68,10 @@ def config_dict(storage, L=LBOX):
                         f"R={int(40 * L / 256)}, width 3, sigma 0.03",
             "box": [L, L, L], "lattice": "D3Q27", "highorder": True, "twocomponent": True, "densratio": True,
             "storage": storage, "bytes_per_lup": B_LUP[storage],
-            "l2_policy": "state (%.2f GB) larger than the 126 MB L2; no flush" % (L ** 3 * B_LUP[storage] / 1e9)}
+            "l2_policy": ("state (%.2f GB) larger than the 126 MB L2; no flush" % (L ** 3 * B_LUP[storage] / 1e9)
+                          if L ** 3 * B_LUP[storage] / 2 > 126e6 else
+                          "state (%.3f GB) fits in the 126 MB L2: not a valid headline size" %
+                          (L ** 3 * B_LUP[storage] / 1e9))}
 
 
 class ClockSampler:

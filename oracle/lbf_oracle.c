@@ -177,6 +177,23 @@ static void build_tables(orc_state *s)
     }
 }
 
+/* The link table of a lattice as the oracle builds it: returns the number of
+ * links (0 for an unknown lattice) and fills ex, ey, ez, opp, w (27 each). */
+int orc_lattice_table(int lattice, int *ex, int *ey, int *ez, int *opp, double *w)
+{
+    orc_state s;
+    int l;
+    if (lattice != 15 && lattice != 19 && lattice != 27) return 0;
+    memset(&s, 0, sizeof(s));
+    s.p.lattice = lattice;
+    build_tables(&s);
+    for (l = 0; l < s.nl; l++) {
+        ex[l] = s.ex[l]; ey[l] = s.ey[l]; ez[l] = s.ez[l]; opp[l] = s.opp[l];
+        w[l] = (double)s.w[l];
+    }
+    return s.nl;
+}
+
 void orc_minv_table(double *out /* 27*27, out[r*27+l] */)
 {
     orc_state s;

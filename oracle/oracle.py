@@ -66,6 +66,9 @@ def _lib(prec: str) -> C.CDLL:
         lib.orc_get_step.restype = C.c_long
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_minv_table.argtypes = [dp]
+        ip = C.POINTER(C.c_int)
+        lib.orc_lattice_table.argtypes = [C.c_int, ip, ip, ip, ip, dp]
+        lib.orc_lattice_table.restype = C.c_int
         _libs[prec] = lib
     return _libs[prec]
 
@@ -77,6 +80,17 @@ def _dp(a: np.ndarray):
 def minv_table() -> np.ndarray:
     out = np.zeros((27, 27), dtype=np.float64)
     _lib("f64").orc_minv_table(_dp(out))
+    return out
+
+
+def lattice_table(lattice: int) -> dict:
+    """ex, ey, ez, opp, w of a lattice as the oracle builds them."""
+    a = {k: np.zeros(27, dtype=np.int32) for k in ("ex", "ey", "ez", "opp")}
+    w = np.zeros(27, dtype=np.float64)
+    ip = lambda v: v.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+    n = _lib("f64").orc_lattice_table(int(lattice), ip(a["ex"]), ip(a["ey"]), ip(a["ez"]), ip(a["opp"]), _dp(w))
+    out = {k: v[:n].tolist() for k, v in a.items()}
+    out["w"] = w[:n].tolist()
     return out
 
 

@@ -1,6 +1,7 @@
 """The CPU oracle against what pins it: the reference's Minv_mrt table, the
 reference's analytic Taylor-Green check (statistics.f90:918-956), and the
 invariants of the scheme.  No GPU."""
+import json
 import os
 
 import numpy as np
@@ -134,3 +135,21 @@ def test_smagorinsky_changes_the_relaxation(name):
     fl = np.abs(isf) == 1
     assert np.all(np.isfinite(out[1][:, fl]))
     assert rel_l2(out[1], out[0], fl) > 1e-6
+
+
+@pytest.mark.parametrize("lattice", [27, 19, 15])
+def test_lattice_tables_match_the_reference(lattice):
+    """Link vectors, opposites and weights of D3Q27 / D3Q19 / D3Q15 as the
+    reference defines them (vars_module.f90:319-338, 666-684, 685-703; parsed
+    into tests/golden/lattice_tables.json by make_lattice_golden.py), and
+    D3Q19 / D3Q15 as subsets of the D3Q27 order (links 0-18; 0-6 and 19-26),
+    which the kernels and the host code rely on."""
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "lattice_tables.json")))[str(lattice)]
+    t = O.lattice_table(lattice)
+    assert t["ex"] == g["ex"] and t["ey"] == g["ey"] and t["ez"] == g["ez"] and t["opp"] == g["opp"]
+    assert np.allclose(t["w"], g["w"], rtol=1e-15, atol=0)
+    g27 = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "lattice_tables.json")))["27"]
+    sub = list(range(27)) if lattice == 27 else list(range(19)) if lattice == 19 else list(range(7)) + list(range(19, 27))
+    assert [g27["ex"][l] for l in sub] == g["ex"]
+    assert [g27["ey"][l] for l in sub] == g["ey"]
+    assert [g27["ez"][l] for l in sub] == g["ez"]
