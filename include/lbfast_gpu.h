@@ -149,7 +149,9 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press);
  * (mass) and of u, v, w (momentum), computed on the device.
  * Counterpart of the reference's phi_sum_count_kernel
  * (lb_cuda_boundary_module.f90:461-515) and sum_world_float
- * (mpi_module.f90:7491-7560) on one rank.  out[5] = {phi, P, u, v, w}. */
+ * (mpi_module.f90:7491-7560) on one rank.  out[5] = {phi, P, u, v, w}.
+ * Returns LBF_E_NUMERIC (with the sums written) when a sum is not finite:
+ * the check a driver calls every few steps to stop a run that blew up. */
 int lbf_reduce(lbf_handle* h, double out[5]);
 
 /* ---- allocation-free reduction ----

@@ -714,6 +714,10 @@ int lbf_reduce(lbf_handle* h, double out[5]) {
                                 h->obs ? h->isf : nullptr, inv, h->d_red, h->stream));
     CUDA_TRY(cudaMemcpyAsync(out, h->d_red, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < 5; ++k)
+        if (!std::isfinite(out[k]))
+            return fail(LBF_E_NUMERIC, "lbf_reduce: the sum of %s over the fluid is not finite at step %lld",
+                        k == 0 ? "phi" : k == 1 ? "P" : k == 2 ? "u" : k == 3 ? "v" : "w", h->step);
     return LBF_OK;
 }
 

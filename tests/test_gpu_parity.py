@@ -138,3 +138,19 @@ def test_schedule_does_not_change_results(name, storage):
     assert rel_l2(m8, ref[0], fl) < bar
     if ref[1] is not None:
         assert rel_l2(p8, ref[1], fl) < bar
+
+
+
+def test_reduce_reports_non_finite_state():
+    """lbf_reduce returns LBF_E_NUMERIC when a sum over the fluid is not finite."""
+    from lbfast_b200.capi import LbfError
+    p, isf, m, phi = make_case("q27ho_2c_dr", "f32")
+    m = m.copy()
+    m[1, 3, 4, 5] = np.nan
+    s = Solver(p)
+    s.set_fields(m, phi)
+    s.step(2)
+    with pytest.raises(LbfError) as e:
+        s.reduce()
+    assert e.value.code == -7 and "not finite" in str(e.value)
+    s.close()
