@@ -24,7 +24,7 @@ LBF_F32, LBF_F64 = 0, 1
 EXPORTED = (
     "lbf_version", "lbf_last_error", "lbf_create", "lbf_destroy", "lbf_set_stream", "lbf_set_isfluid",
     "lbf_set_fields", "lbf_step", "lbf_sync", "lbf_get_step", "lbf_get_fields", "lbf_get_print_fields",
-    "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet",
+    "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet", "lbf_ic_lamb",
     "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
     "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning", "lbf_write_restart_raw",
     "lbf_read_restart_raw", "lbf_write_vtk",
@@ -93,6 +93,7 @@ def load() -> C.CDLL:
     lib.lbf_seed_solid_phi.argtypes = [C.c_int] * 4 + [i8p, dp]
     lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
     lib.lbf_ic_droplet.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
+    lib.lbf_ic_lamb.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
     lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
     lib.lbf_write_vtk.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
     lib.lbf_write_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, C.c_int, C.c_int]
@@ -383,6 +384,18 @@ def ic_droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio
     check(load().lbf_ic_droplet(lx, ly, lz, _ptr(c, C.c_double), float(radius), float(width), float(sigma),
                                 float(rho_r), float(rho_b), int(densratio), _ptr(i, C.c_int8),
                                 _ptr(m, C.c_double), _ptr(phi, C.c_double)))
+    return m, phi
+
+
+def ic_lamb(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio=True, isf=None):
+    """LAMBTEST initial droplet: as ic_droplet with the x distance halved."""
+    m = np.empty((10, lz, ly, lx), dtype=np.float64)
+    phi = np.empty((lz, ly, lx), dtype=np.float64)
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    i = None if isf is None else np.ascontiguousarray(isf, dtype=np.int8)
+    check(load().lbf_ic_lamb(lx, ly, lz, _ptr(c, C.c_double), float(radius), float(width), float(sigma),
+                             float(rho_r), float(rho_b), int(densratio), _ptr(i, C.c_int8), _ptr(m, C.c_double),
+                             _ptr(phi, C.c_double)))
     return m, phi
 
 

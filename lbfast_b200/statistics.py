@@ -7,6 +7,12 @@ copy_print fields (rho with PRINTPHI = phi, vel, press) a run returns.
   sigma_eff = delta_p * radius / 2.
 * Taylor-Green (statistics.f90:36-86, 918-956): mean kinetic energy and the
   viscosity fitted to E/E0 = exp(-6 nu k^2 t).
+* Poiseuille (statistics.f90:825-880): the velocity along z averaged over each
+  x plane, against fz / (2 nu) (H^2 - d^2).
+* Lamb (statistics.f90:377-471, 959-1100): phi(1-phi)-weighted interface
+  positions along the x and z lines through the box centre, the z half-axis
+  (the reference's `dosc`), and Lamb's n = 2 frequency with the reference's
+  viscous correction.
 Indices follow the reference's 1-based global coordinates.
 """
 from __future__ import annotations
@@ -61,3 +67,70 @@ def fit_viscosity(steps, energies, L: int) -> float:
     k = 2.0 * np.pi / L
     slope = np.polyfit(t, np.log(e / e[0]), 1)[0]
     return -slope / (6.0 * k * k)
+
+
+def poiseuille_profile(w, isf):
+    """statistics.f90:842-868: w (lz, ly, lx) velocity along z, 0 on solid
+    nodes, averaged over each x plane (gi = 1..lx)."""
+    w = np.where(np.asarray(isf) == 0, 0.0, np.asarray(w, dtype=np.float64))
+    return w.mean(axis=(0, 1))
+
+
+def poiseuille_theory(lx: int, fz: float, nu: float, H: float, xc: float):
+    """fz / (2 nu) (H^2 - (gi - xc)^2) inside |gi - xc| <= H, 0 outside
+    (statistics.f90:831-845: H = (lx-1)/2, xc = (lx+1)/2 puts the walls on the
+    solid nodes; H = lx/2 - 1 the half-way walls of bounce-back)."""
+    gi = np.arange(1, lx + 1, dtype=np.float64)
+    d = np.abs(gi - xc)
+    return np.where(d <= H, fz / (2.0 * nu) * (H * H - d * d), 0.0)
+
+
+def _interface_pos(line, idx):
+    w = line * (1.0 - line)
+    return float((idx * w).sum() / w.sum())
+
+
+def lamb_observables(phi):
+    """print_lamb (statistics.f90:377-471): interface positions along the x
+    line (gj = ly/2, gk = lz/2) and the z line (gi = lx/2, gj = ly/2), each
+    half separately.  Returns (lamb_x, lamb_z, dosc) with lamb_* the extents
+    and dosc = z half-axis (pos_z_right - centre), the series the reference's
+    frequency analysis reads."""
+    phi = np.asarray(phi, dtype=np.float64)
+    lz, ly, lx = phi.shape
+    gi, gj, gk = lx // 2, ly // 2, lz // 2
+    zl = phi[:, gj - 1, gi - 1]
+    xl = phi[gk - 1, gj - 1, :]
+    kz = np.arange(1, lz + 1, dtype=np.float64)
+    kx = np.arange(1, lx + 1, dtype=np.float64)
+    zlo, zhi = _interface_pos(zl[: lz // 2], kz[: lz // 2]), _interface_pos(zl[lz // 2:], kz[lz // 2:])
+    xlo, xhi = _interface_pos(xl[: lx // 2], kx[: lx // 2]), _interface_pos(xl[lx // 2:], kx[lx // 2:])
+    lamb_z, lamb_x = zhi - zlo, xhi - xlo
+    return lamb_x, lamb_z, zhi - 0.5 * (zhi + zlo)
+
+
+def lamb_theory_omega(sigma, radius, rho_r, rho_b, visc1, visc2):
+    """statistics.f90:973-981: Lamb's n = 2 angular frequency of a droplet
+    (density rho_r) in a host fluid (rho_b), with the reference's viscous
+    correction."""
+    mu1, mu2 = rho_r * visc1, rho_b * visc2
+    w0 = np.sqrt(24.0 * sigma / (radius ** 3 * (2.0 * rho_b + 3.0 * rho_r)))
+    chi = ((2 * 2 + 1) ** 2 * np.sqrt(mu1 * mu2 * rho_r * rho_b)) / (
+        np.sqrt(2.0) * radius * (2.0 * rho_b + 3.0 * rho_r) * (np.sqrt(mu1 * rho_r) + np.sqrt(mu2 * rho_b)))
+    return w0 - 0.5 * chi * np.sqrt(w0) + 0.25 * chi ** 2
+
+
+def mean_period(steps, series, min_dist: float):
+    """Mean distance between the local maxima of `series` above its mean that
+    are at least min_dist apart (statistics.f90:1020-1050)."""
+    s = np.asarray(series, dtype=np.float64)
+    t = np.asarray(steps, dtype=np.float64)
+    ref = s.mean()
+    peaks = []
+    for i in range(1, len(s) - 1):
+        if s[i] > s[i - 1] and s[i] >= s[i + 1] and s[i] > ref:
+            if not peaks or t[i] - peaks[-1] >= min_dist:
+                peaks.append(t[i])
+    if len(peaks) < 2:
+        return float("nan"), len(peaks)
+    return float(np.mean(np.diff(peaks))), len(peaks)
