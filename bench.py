@@ -46,9 +46,8 @@ UNIT = "MLUPS"
 LBOX = 256
 RHO_R, RHO_B = 100.0, 1.0
 B_LUP = {"f32": 112, "f16": 64, "bf16": 64, "f64": 224}  # algorithmic bytes per lattice update
-# DRAM bytes (read + write) of one step launch from one ncu capture at this
-# workload: profiles/stream_kernel_laplace256_f32.md and
-# profiles/stream_kernel_laplace256_full.md
+# DRAM bytes (read + write) of one step launch of the tuned kernel, measured
+# by ncu (dram__bytes_read.sum + dram__bytes_write.sum) at this workload
 NCU_TRAFFIC = {("f32", 256): 1845157888}
 
 

@@ -1,7 +1,7 @@
 """ctypes binding of the C ABI in include/lbfast_gpu.h.
 
 This is the Python-side stand-in for the Fortran ``bind(C)`` interface a
-reference driver would use (see INTEGRATION.md): every call goes through the
+reference driver would use: every call goes through the
 same exported C symbols.  The shared library is the in-tree build
 ``lbfast_b200/_lib/liblbfast_b200.so``; there is no fallback -- if it is
 missing or fails to load, importing the solver raises.
