@@ -509,7 +509,10 @@ int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype)
         std::memcpy(&mU, &bits[0], sizeof mU);
         std::memcpy(&mPi, &bits[1], sizeof mPi);
         h->scale[0] = 1.0;
-        for (int f = 1; f <= 3; ++f) h->scale[f] = h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-2);
+        // velocity floor 1e-3: a flow that starts at rest keeps 11 significant
+        // bits down to ~1e-6 and still represents |u| up to 0.5, beyond any
+        // lattice Boltzmann velocity
+        for (int f = 1; f <= 3; ++f) h->scale[f] = h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-3);
         for (int f = 4; f < 10; ++f) h->scale[f] = pick_scale(h->storage, mPi, 1e-4);
         for (int b = 0; b < 2; ++b) {
             CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, dtype, h->pres[b], N, 1.0, h->stream));
