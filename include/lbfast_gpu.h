@@ -53,7 +53,7 @@ enum { LBF_F32 = 0, LBF_F64 = 1 };
 typedef struct lbf_params {
     int lx, ly, lz;          /* box (one GPU: nx = lx etc.) */
     int pbc_x, pbc_y, pbc_z; /* 1 = periodic */
-    int lattice;             /* 19 or 27 */
+    int lattice;             /* 15, 19 or 27 */
     int highorder;           /* HIGHORDER, LATTICE 27 only */
     int twocomponent;        /* TWOCOMPONENT */
     int densratio;           /* DENSRATIO (requires twocomponent) */
@@ -84,6 +84,18 @@ typedef struct lbf_params {
                                 applies with open boundaries only); 0 = off (the reference default) */
     int smagorinsky;         /* SMAGORINSKI: LES relaxation time from the non-equilibrium stress
                                 (lb_cuda_fused_module.f90:609-616, lb_cuda_boundary_module.f90:150-160) */
+    int openbc;              /* openbc = 1 (requires obstacles): open faces on every non-periodic axis, as
+                                bcs_mesoscopic_hfields / _phifields do (boundary_cds_module.f90:57-1663).
+                                At the isfluid = -1 nodes of the plane next to each wall (tangential indices
+                                1 .. l-2) the wall links' bounce-back populations are replaced by those of
+                                the face's state; the wall nodes of the face take the phi of their
+                                neighbour; with phi_correction the mass target moves by the phi carried
+                                through the faces (BCPHIFLUX) */
+    int openbc_type[3][2];   /* per axis (x, y, z) and side (low, high), openbc_type_x/y/z: 2 zero gradient
+                                (the node's own P and u), 1 pressure (openbc_press, the node's u), any other
+                                value velocity (the node's P, openbc_vel) */
+    double openbc_press[3][2];   /* pressure moment P of a pressure face (openbc_press_x/y/z) */
+    double openbc_vel[3][2][3];  /* (u, v, w) of a velocity face (openbc_u/v/w_x/y/z) */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;
@@ -217,8 +229,9 @@ typedef struct lbf_run {
  * (LBFAST.f90:193-232) into p (physics) and run (controls); p->lx..wettab_r
  * and run are first set to the DOBENCHMARK defaults.  The compile-time macro
  * fields of p (lattice, highorder, twocomponent, densratio, obstacles,
- * storage, printphi) are left as the caller set them.  Unknown keys,
- * malformed values and openbc = 1 are errors. */
+ * storage, printphi) are left as the caller set them; openbc and the
+ * openbc_* arrays (whole-array or element assignments) go to both p and run.
+ * Unknown keys and malformed values are errors. */
 int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run);
 
 /* The reference's restart file <dir>/restart.raw (write_restart_serial_2c /

@@ -42,7 +42,8 @@ class LbfParams(C.Structure):
         ("sigma", C.c_double), ("width", C.c_double), ("tau_diff", C.c_double),
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double), ("wettab_r", C.c_double),
         ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int), ("phi_correction", C.c_int),
-        ("smagorinsky", C.c_int),
+        ("smagorinsky", C.c_int), ("openbc", C.c_int), ("openbc_type", (C.c_int * 2) * 3),
+        ("openbc_press", (C.c_double * 2) * 3), ("openbc_vel", ((C.c_double * 3) * 2) * 3),
     ]
 
 
@@ -163,6 +164,13 @@ class Params:
     tile_y: int = 0
     phi_correction: int = 0
     smagorinsky: int = 0
+    # open faces on the non-periodic axes (requires obstacles); per axis
+    # (x, y, z) and side (low, high): type 2 zero gradient, 1 pressure, other
+    # velocity; pressure moment P; velocity (u, v, w)
+    openbc: int = 0
+    openbc_type: tuple = ((0, 0), (0, 0), (0, 0))
+    openbc_press: tuple = ((0.0, 0.0), (0.0, 0.0), (0.0, 0.0))
+    openbc_vel: tuple = (((0.0,) * 3,) * 2,) * 3
 
     def to_c(self) -> LbfParams:
         p = LbfParams()
@@ -170,6 +178,16 @@ class Params:
             v = getattr(self, f.name)
             if f.name == "storage":
                 v = STORE[v]
+            if f.name.startswith("openbc_"):
+                arr = getattr(p, f.name)
+                for a in range(3):
+                    for sd in range(2):
+                        if f.name == "openbc_vel":
+                            for d in range(3):
+                                arr[a][sd][d] = float(v[a][sd][d])
+                        else:
+                            arr[a][sd] = v[a][sd]
+                continue
             setattr(p, f.name, v)
         return p
 

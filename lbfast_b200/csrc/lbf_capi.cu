@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/lbfast_gpu.h"
@@ -200,6 +201,16 @@ int autotune(lbf_handle* h) {
     return LBF_OK;
 }
 
+// phi carried through the open faces by the state of buffer b into d_mass[3]
+// (stays 0 without open faces)
+cudaError_t launch_face_flux(lbf_handle* h, int b) {
+    if (!h->obc_open || !h->tc) return cudaSuccess;
+    double inv[4];
+    for (int f = 0; f < 4; ++f) inv[f] = 1.0 / h->scale[f];
+    return lbf::launch_phi_flux(h->storage, h->nx, h->ny, h->nz, h->obc_open, h->mom[b], h->phi[b], h->isf, inv,
+                                h->d_mass + 3, h->stream);
+}
+
 // Pre-loop wetting of integrator_module.f90:186-190 / one launch per step.
 int launch_wet(lbf_handle* h, int in_buf, int out_buf, bool prime) {
     if (!(h->tc && h->obs) || h->nwet == 0) return LBF_OK;
@@ -255,6 +266,12 @@ int prime(lbf_handle* h) {
                                   h->stream));
     int rc = launch_wet(h, h->cur, 1 - h->cur, true);
     if (rc) return rc;
+    // with open faces the pre-loop bcs_mesoscopic_phifields corrects once with
+    // the flux of the initial state (integrator_module.f90:179-182)
+    if (h->d_mass && h->obc_open) {
+        CUDA_TRY(launch_face_flux(h, h->cur));
+        CUDA_TRY(lbf::launch_mass(h->storage, false, h->N, h->phi[h->cur], h->isf, h->d_mass, h->stream));
+    }
     h->primed = true;
     return LBF_OK;
 }
@@ -300,6 +317,11 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (p->twocomponent && (p->width <= 0)) return fail(LBF_E_ARG, "interface width must be positive");
     if (p->densratio && (p->rho_r <= 0 || p->rho_b <= 0)) return fail(LBF_E_ARG, "densities must be positive");
     if (p->phi_correction && !p->twocomponent) return fail(LBF_E_ARG, "phi_correction requires TWOCOMPONENT");
+    // bcs_mesoscopic_hfields / _phifields run only with INTERNAL_OBSTACLES (integrator_module.f90:514-523)
+    if (p->openbc && !p->obstacles) return fail(LBF_E_ARG, "openbc requires obstacles (INTERNAL_OBSTACLES)");
+    // an open axis holds a wall, the face plane and a wall at least
+    if (p->openbc && ((!p->pbc_x && p->lx < 3) || (!p->pbc_y && p->ly < 3) || (!p->pbc_z && p->lz < 3)))
+        return fail(LBF_E_ARG, "openbc: a non-periodic axis needs at least 3 nodes");
     lbf_handle* h = new (std::nothrow) lbf_handle();
     if (!h) return fail(LBF_E_NOMEM, "host allocation failed");
     h->p = *p;
@@ -354,7 +376,8 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (ok && h->obs) ok = cudaMalloc(&h->isf, h->N) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_red, 5 * sizeof(double)) == cudaSuccess;
-    if (ok && p->phi_correction) ok = cudaMalloc(&h->d_mass, 3 * sizeof(double)) == cudaSuccess;
+    if (ok && p->phi_correction) ok = cudaMalloc(&h->d_mass, 4 * sizeof(double)) == cudaSuccess;
+    if (p->openbc) h->obc_open = (p->pbc_x ? 0 : 1) | (p->pbc_y ? 0 : 2) | (p->pbc_z ? 0 : 4);
     if (!ok) {
         cudaGetLastError();
         free_all(h);
@@ -364,6 +387,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     }
     cudaMemset(h->d_err, 0, sizeof(int));
     if (h->obs) cudaMemset(h->isf, 1, h->N);
+    if (h->d_mass) cudaMemset(h->d_mass, 0, 4 * sizeof(double));
     *out = h;
     return LBF_OK;
 }
@@ -461,6 +485,40 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
                 vwn.insert(vwn.end(), {wx, wy, wz});
                 vsh.insert(vsh.end(), {-EXh[bl], -EYh[bl], -EZh[bl]});
             }
+    // open faces: the wall nodes of each face (tangential indices 1 .. n-2)
+    // take the phi of their neighbour on the plane next to them after the
+    // wetting (boundary_cds_module.f90:1351-1663): entries of the same list
+    if (h->obc_open) {
+        std::unordered_map<long long, size_t> at;
+        for (size_t e = 0; e < vs.size(); ++e) at[vs[e]] = e;
+        for (int axis = 0; axis < 3; ++axis) {
+            if (!(h->obc_open & (1 << axis))) continue;
+            const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+            for (int side = 0; side < 2; ++side)
+                for (int t2 = 1; t2 <= dims[a2] - 2; ++t2)
+                    for (int t1 = 1; t1 <= dims[a1] - 2; ++t1) {
+                        int w[3], d[3];
+                        w[axis] = side ? dims[axis] - 1 : 0; w[a1] = t1; w[a2] = t2;
+                        d[axis] = side ? dims[axis] - 2 : 1; d[a1] = t1; d[a2] = t2;
+                        const long long c = ((long long)w[2] * ny + w[1]) * nx + w[0];
+                        auto it = at.find(c);
+                        size_t e;
+                        if (it == at.end()) {
+                            e = vs.size();
+                            at[c] = e;
+                            vs.push_back(c);
+                            vd.insert(vd.end(), {0, 0, 0});
+                            vf.push_back(0);
+                            vwn.insert(vwn.end(), {0.0, 0.0, 0.0});
+                            vsh.insert(vsh.end(), {0, 0, 0});
+                        } else {
+                            e = it->second;
+                        }
+                        vf[e] = lbf::WET_OPENCOPY;
+                        vd[3 * e] = d[0]; vd[3 * e + 1] = d[1]; vd[3 * e + 2] = d[2];
+                    }
+        }
+    }
     cudaFree(h->wet_s); cudaFree(h->wet_donor); cudaFree(h->wet_flag); cudaFree(h->wet_wn); cudaFree(h->wet_shift);
     cudaFree(h->wetW[0]); cudaFree(h->wetW[1]);
     h->wet_s = nullptr; h->wet_donor = nullptr; h->wet_flag = nullptr; h->wet_wn = nullptr; h->wet_shift = nullptr;
@@ -767,14 +825,43 @@ size_t handle_bytes(const lbf_params* p) {
     if (p->twocomponent) b += 2 * N * psz;
     if (half) b += 2 * N * sizeof(float);
     if (p->obstacles) b += N;
-    if (p->phi_correction) b += 3 * sizeof(double);
+    if (p->phi_correction) b += 4 * sizeof(double);
     return b;
 }
 
 int handle_pre_step(lbf_handle* h) { return launch_wet(h, h->cur, 1 - h->cur, false); }
 
 int handle_post_step(lbf_handle* h) {
+    // open faces on the step's output moments (buffer cur after the advance),
+    // from the step's input buffers (1 - cur), which the step left intact
+    if (h->obc_open) {
+        const int in = 1 - h->cur;
+        lbf::OpenFaceArgs a;
+        a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+        a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
+        a.lattice = h->p.lattice; a.highorder = h->p.highorder; a.tc = h->tc; a.dr = h->dr;
+        a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
+        a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
+        a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;
+        a.fx = h->p.fx; a.fy = h->p.fy; a.fz = h->p.fz;
+        a.isf = h->isf;
+        a.min = h->mom[in]; a.pres_in = h->pres[in]; a.uin = h->uold[in];
+        a.phi = h->tc ? h->phi[in] : nullptr;
+        a.mom = h->mom[h->cur]; a.pres = h->pres[h->cur];
+        for (int f = 0; f < lbf::NSCALE_H; ++f) a.scale[f] = h->scale[f];
+        for (int axis = 0; axis < 3; ++axis) {
+            if (!(h->obc_open & (1 << axis))) continue;
+            for (int side = 0; side < 2; ++side) {
+                a.axis = axis; a.side = side;
+                a.type = h->p.openbc_type[axis][side];
+                a.press = h->p.openbc_press[axis][side];
+                for (int d = 0; d < 3; ++d) a.vel[d] = h->p.openbc_vel[axis][side][d];
+                CUDA_TRY(lbf::launch_open_face(h->storage, a, h->stream));
+            }
+        }
+    }
     if (!h->d_mass) return LBF_OK;
+    CUDA_TRY(launch_face_flux(h, h->cur));
     CUDA_TRY(lbf::launch_mass(h->storage, false, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass, h->stream));
     return LBF_OK;
 }

@@ -45,7 +45,8 @@ struct lbf_handle {
     lbf::StepLauncher launcher = nullptr;
     int zseg = 0;
     int tile_y = 8;      // rows of the kernel tile
-    double* d_mass = nullptr;  // phi correction: {sum, count, sum at the first step} (FP64)
+    double* d_mass = nullptr;  // phi correction: {sum, count, sum at the first step, face flux} (FP64)
+    int obc_open = 0;  // open faces (openbc, non-periodic axes): bit 0 x, 1 y, 2 z
     bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
 };
 

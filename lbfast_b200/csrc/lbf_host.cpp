@@ -245,9 +245,16 @@ struct NmlError {
     std::string msg;
 };
 
+// one assignment: key, raw values, first element index (key(i) = ..., 1 otherwise)
+struct NmlItem {
+    std::string first;
+    std::vector<std::string> second;
+    int idx;
+};
+
 // split "a = 1, b = 2.0" style text into key -> list of raw values
-std::vector<std::pair<std::string, std::vector<std::string>>> parse_group(const std::string& body) {
-    std::vector<std::pair<std::string, std::vector<std::string>>> out;
+std::vector<NmlItem> parse_group(const std::string& body) {
+    std::vector<NmlItem> out;
     // tokens separated by commas / whitespace; a key is a token followed by '='
     std::string s = body;
     for (char& c : s)
@@ -255,10 +262,12 @@ std::vector<std::pair<std::string, std::vector<std::string>>> parse_group(const 
     size_t i = 0;
     std::string key;
     std::vector<std::string> vals;
+    int idx = 1;
     auto flush = [&]() {
-        if (!key.empty()) out.push_back({key, vals});
+        if (!key.empty()) out.push_back({key, vals, idx});
         key.clear();
         vals.clear();
+        idx = 1;
     };
     while (i < s.size()) {
         while (i < s.size() && (s[i] == ' ' || s[i] == ',')) ++i;
@@ -272,7 +281,15 @@ std::vector<std::pair<std::string, std::vector<std::string>>> parse_group(const 
             flush();
             key = lower(tok);
             size_t p = key.find('(');
-            if (p != std::string::npos) key = key.substr(0, p);  // element assignment key(1)=
+            if (p != std::string::npos) {  // element assignment key(i)=
+                const size_t q = key.find(')');
+                const std::string e = key.substr(p + 1, q == std::string::npos ? std::string::npos : q - p - 1);
+                char* end = nullptr;
+                const long v = std::strtol(e.c_str(), &end, 10);
+                if (end == e.c_str() || *end != '\0') throw NmlError{"bad element index in `" + tok + "`"};
+                idx = (int)v;
+                key = key.substr(0, p);
+            }
             i = k + 1;
         } else {
             if (key.empty()) throw NmlError{"value `" + tok + "` without a key"};
@@ -360,6 +377,13 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
     p->width = 0.0;
     p->tau_diff = 0.0;
     p->wettab_r = 90.0;
+    p->openbc = 0;  // vars_module.f90:238-255
+    for (int a = 0; a < 3; ++a)
+        for (int sd = 0; sd < 2; ++sd) {
+            p->openbc_type[a][sd] = 0;
+            p->openbc_press[a][sd] = 0.0;
+            for (int d = 0; d < 3; ++d) p->openbc_vel[a][sd][d] = 0.0;
+        }
     try {
         for (auto& kv : parse_group(group_body(text, "simulation"))) {
             const std::string& k = kv.first;
@@ -384,7 +408,7 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
             else if (k == "pbc_x") p->pbc_x = to_int(a, k);
             else if (k == "pbc_y") p->pbc_y = to_int(a, k);
             else if (k == "pbc_z") p->pbc_z = to_int(a, k);
-            else if (k == "openbc") run->openbc = to_int(a, k);
+            else if (k == "openbc") { run->openbc = to_int(a, k); p->openbc = run->openbc; }
             else if (k == "iprobe") run->iprobe = to_int(a, k);
             else if (k == "jprobe") run->jprobe = to_int(a, k);
             else if (k == "kprobe") run->kprobe = to_int(a, k);
@@ -392,8 +416,22 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
             else if (k == "time_limit") run->time_limit = to_real(a, k);
             else if (k == "every_time_check") run->every_time_check = to_int(a, k);
             else if (k == "lasync" || k == "lweakscaling") to_bool(a, k);
-            else if (k.rfind("openbc_type_", 0) == 0) { for (auto& x : v) to_int(x, k); }
-            else if (k.rfind("openbc_", 0) == 0) { for (auto& x : v) to_real(x, k); }
+            else if (k.rfind("openbc_", 0) == 0 && k.size() >= 9 && k[k.size() - 2] == '_' &&
+                     (k.back() == 'x' || k.back() == 'y' || k.back() == 'z')) {
+                // openbc_type_x(2), openbc_press_y(2), openbc_u_z(2), ... (vars_module.f90:240-255)
+                const int axis = k.back() - 'x';
+                const std::string what = k.substr(7, k.size() - 9);
+                for (size_t m = 0; m < v.size(); ++m) {
+                    const int side = kv.idx - 1 + (int)m;
+                    if (side < 0 || side > 1) throw NmlError{"element out of range (1:2) for " + k};
+                    if (what == "type") p->openbc_type[axis][side] = to_int(v[m], k);
+                    else if (what == "press") p->openbc_press[axis][side] = to_real(v[m], k);
+                    else if (what == "u") p->openbc_vel[axis][side][0] = to_real(v[m], k);
+                    else if (what == "v") p->openbc_vel[axis][side][1] = to_real(v[m], k);
+                    else if (what == "w") p->openbc_vel[axis][side][2] = to_real(v[m], k);
+                    else throw NmlError{"unknown key `" + k + "` in &simulation"};
+                }
+            }
             else throw NmlError{"unknown key `" + k + "` in &simulation"};
         }
         bool have_radius = false;
@@ -428,10 +466,6 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
     } catch (const NmlError& e) {
         std::fprintf(stderr, "lbf_read_namelists: %s: %s\n", path, e.msg.c_str());
         return LBF_E_ARG;
-    }
-    if (run->openbc != 0) {
-        std::fprintf(stderr, "lbf_read_namelists: openbc = %d: open boundaries are not supported\n", run->openbc);
-        return LBF_E_UNSUPPORTED;
     }
     return LBF_OK;
 }

@@ -69,7 +69,7 @@ struct WetArgs {
     const void* scatter_src;  // ghost values of the previous step
     int prime;                // integrator pre-loop call: aux = 0 and halos = 0
 };
-enum { WET_NORMAL = 0, WET_OUTSIDE = 1, WET_HIGHWRAP = 2 };
+enum { WET_NORMAL = 0, WET_OUTSIDE = 1, WET_HIGHWRAP = 2, WET_OPENCOPY = 3 };
 
 cudaError_t launch_wetting(int storage, const WetArgs& a, cudaStream_t st);
 cudaError_t launch_wet_apply(int storage, int n, const long long* s_idx, const void* src, void* dst, cudaStream_t st);
@@ -113,10 +113,41 @@ cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const vo
 
 // phi mass correction: initial == true stores the FP64 sum of phi over fluid
 // nodes in d_mass[2]; otherwise the sum and the count of 0.5 < phi < 0.9 go to
-// d_mass[0..1] and (d_mass[2] - sum) / count is added to those nodes.  No host
-// synchronisation (graph-capturable).
+// d_mass[0..1] and (d_mass[2] + d_mass[3] - sum) / count is added to those
+// nodes, d_mass[3] the open-face flux of the state (0 without open faces).
+// No host synchronisation (graph-capturable).
 cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
                         cudaStream_t st);
+
+// Open face (axis 0/1/2, side 0 low / 1 high) after a step: replaces the
+// bounce-back populations of the wall links at the face's isfluid = -1 nodes
+// by those of the face's state, on the step's output moments
+// (boundary_cds_module.f90:57-1311).  The face nodes' moments after the force
+// half-step are recomputed from the step's input buffers, which the step
+// leaves intact.  One launch per face, in the reference's order x low,
+// x high, y low, ..., z high.
+struct OpenFaceArgs {
+    int nx, ny, nz, pbx, pby, pbz;
+    int axis, side, type;       // type: 2 zero gradient, 1 pressure, other velocity
+    double press, vel[3];
+    int lattice, highorder, tc, dr;
+    double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
+    const int8_t* isf;
+    const void* min;            // the step's input moments
+    const float* pres_in;       // the step's input P (16-bit storage)
+    const void* uin;            // the step's input u_old (DENSRATIO)
+    const void* phi;            // the step's input phi (two components)
+    void* mom;                  // the step's output moments
+    float* pres;                // the step's output P (16-bit storage)
+    double scale[NSCALE_H];
+};
+cudaError_t launch_open_face(int storage, const OpenFaceArgs& a, cudaStream_t st);
+
+// phi carried through the open faces by a state (BCPHIFLUX,
+// boundary_cds_module.f90:1667-1861): sum over the isfluid = -1 nodes of the
+// planes next to the walls of +-u_n phi, into d_flux (set, not added)
+cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const void* phi,
+                            const int8_t* isf, const double* inv_scale, double* d_flux, cudaStream_t st);
 
 size_t storage_bytes(int storage);
 

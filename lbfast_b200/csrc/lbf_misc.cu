@@ -57,8 +57,16 @@ __global__ void wetting_kernel(const WetArgs a) {
         if (a.scatter_dst) {
             static_cast<SP*>(a.scatter_dst)[a.s_idx[i]] = static_cast<const SP*>(a.scatter_src)[i];
         }
-        const R old = CP::ld(pin, a.s_idx[i], R(1));
         const int flag = a.flag[i];
+        if (flag == WET_OPENCOPY) {
+            // wall node of an open face: the phi of its neighbour on the plane
+            // next to it replaces the wetting value (boundary_cds_module.f90:1351-1663)
+            const long long d = (long long)a.donor[3 * i + 2] * plane + (long long)a.donor[3 * i + 1] * a.nx +
+                                a.donor[3 * i];
+            wout[i] = pin[d];
+            continue;
+        }
+        const R old = CP::ld(pin, a.s_idx[i], R(1));
         R ghost;
         if (flag == WET_OUTSIDE || (a.prime && flag == WET_HIGHWRAP)) {
             // donor on a never-written halo layer: phi = 0 and aux = 0 there
@@ -387,7 +395,7 @@ __global__ void mass_sum_kernel(long long N, const SP* phi, const int8_t* isf, d
 template <typename SP>
 __global__ void mass_apply_kernel(long long N, SP* phi, const int8_t* isf, const double* m) {
     if (m[1] <= 0.0) return;
-    const double corr = (m[2] - m[0]) / m[1];
+    const double corr = (m[2] + m[3] - m[0]) / m[1];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         if (isf) {
             const int f = isf[i];

@@ -1,0 +1,368 @@
+// lbf_openbc.cu -- open faces of the reference's bcs_mesoscopic_hfields
+// (boundary_cds_module.f90:57-1311) and the phi they carry (BCPHIFLUX,
+// :1667-1861).  The faces touch only the planes next to the walls, so they
+// run as small kernels after the fused step, as the reference runs them after
+// its obstacle pass.  A face node needs its moments after the force half-step,
+// which the fused step holds only in registers; the face kernel recomputes
+// them from the step's input buffers (left intact by the step), so the fused
+// step carries no code for the faces.
+#include <type_traits>
+
+#include "lbf_internal.h"
+#include "lbf_lattice.cuh"
+#include "lbf_stream.cuh"
+
+namespace lbf {
+namespace {
+
+template <typename Fn> cudaError_t by_storage(int storage, Fn&& fn) {
+    switch (storage) {
+        case 0: return fn(float{});
+        case 1: return fn(__half{});
+        case 2: return fn(__nv_bfloat16{});
+        case 3: return fn(double{});
+    }
+    return cudaErrorInvalidValue;
+}
+
+int grid_for(long long n, int bs) {
+    long long b = (n + bs - 1) / bs;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// factor of axis multiplicity m of the D3Q27 Hermite row r in Minv_mrt(r, l)
+// = w_l prod_axes F(m, c): 1, c / cs^2, (c^2 - cs^2) / (2 cs^4)
+__device__ __forceinline__ double hfac(int m, int c) {
+    return m == 0 ? 1.0 : m == 1 ? 3.0 * c : 4.5 * ((double)(c * c) - 1.0 / 3.0);
+}
+
+// axis multiplicities of the rows 10..26 of Minv_mrt (vars_module.f90:360-521)
+__device__ __constant__ int c_hmul[17][3] = {
+    {2, 1, 0}, {2, 0, 1}, {1, 2, 0}, {1, 0, 2}, {0, 1, 2}, {0, 2, 1}, {1, 1, 1}, {2, 2, 0}, {2, 0, 2},
+    {0, 2, 2}, {1, 1, 2}, {1, 2, 1}, {2, 1, 1}, {2, 1, 2}, {2, 2, 1}, {1, 2, 2}, {2, 2, 2}};
+
+// The node's moments after the force half-step (P, u, v, w, Pi), as the
+// moments kernel leaves them (lb_cuda_moments_module.f90:104-339), with the
+// phase-field inputs of compute_norm (lb_cuda_auxfields_module.f90:72-135) and
+// div theta (:1136-1157) at the node: FP64, the 27-point stencils in full.
+template <typename S>
+__device__ void face_node_moments(const OpenFaceArgs& a, int x, int y, int z, long long g, double (&m)[10],
+                                  double& phi_c) {
+    using SP = typename PhiStore<S>::type;
+    using CD = Codec<S>;
+    const long long plane = (long long)a.nx * a.ny, N = plane * a.nz;
+    const S* min = static_cast<const S*>(a.min);
+    const double cssq = 1.0 / 3.0;
+    double P;
+    if constexpr (CD::scaled) P = a.pres_in[g];
+    else P = (double)CD::ld(min, g, 1.0);
+    double u = (double)CD::ld(min + N, g, 1.0 / a.scale[1]);
+    double v = (double)CD::ld(min + 2 * N, g, 1.0 / a.scale[2]);
+    double w = (double)CD::ld(min + 3 * N, g, 1.0 / a.scale[3]);
+    double pi[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) pi[f] = (double)CD::ld(min + (4 + f) * N, g, 1.0 / a.scale[4 + f]);
+    if constexpr (CD::scaled) {  // 16-bit storage keeps Pi - u u
+        pi[0] += u * u; pi[1] += v * v; pi[2] += w * w;
+        pi[3] += u * v; pi[4] += u * w; pi[5] += v * w;
+    }
+    double phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
+    if (a.tc) {
+        const SP* ph = static_cast<const SP*>(a.phi);
+        // phi beyond a non-periodic face is 0 (never-written halo)
+        auto PHI = [&](int i, int j, int k) -> double {
+            bool ok = true;
+            const int xx = wrap_coord(i, a.nx, a.pbx, ok), yy = wrap_coord(j, a.ny, a.pby, ok);
+            const int zz = wrap_coord(k, a.nz, a.pbz, ok);
+            return ok ? (double)ph[(long long)zz * plane + (long long)yy * a.nx + xx] : 0.0;
+        };
+        // theta = phi (1 - phi) n on fluid nodes, 0 elsewhere and beyond non-periodic faces
+        double th[3][3][3][3];
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int i = x + dx, j = y + dy, k = z + dz;
+                    bool ok = true;
+                    const int xx = wrap_coord(i, a.nx, a.pbx, ok), yy = wrap_coord(j, a.ny, a.pby, ok);
+                    const int zz = wrap_coord(k, a.nz, a.pbz, ok);
+                    double t0 = 0, t1 = 0, t2 = 0;
+                    if (ok) {
+                        const int f = a.isf[(long long)zz * plane + (long long)yy * a.nx + xx];
+                        if (f == 1 || f == -1) {
+                            double gx, gy, gz;
+                            iso_grad<double>([&](int p, int q, int r) { return PHI(i + p, j + q, k + r); }, gx, gy, gz);
+                            const double mg = sqrt(gx * gx + gy * gy + gz * gz);
+                            const double den = mg + 1.0e-9;
+                            const double c0 = PHI(i, j, k);
+                            t0 = c0 * (1.0 - c0) * (gx / den);
+                            t1 = c0 * (1.0 - c0) * (gy / den);
+                            t2 = c0 * (1.0 - c0) * (gz / den);
+                            if (dx == 0 && dy == 0 && dz == 0) {
+                                gfx = (gx / den) * mg; gfy = (gy / den) * mg; gfz = (gz / den) * mg;
+                            }
+                        }
+                    }
+                    th[0][dz + 1][dy + 1][dx + 1] = t0;
+                    th[1][dz + 1][dy + 1][dx + 1] = t1;
+                    th[2][dz + 1][dy + 1][dx + 1] = t2;
+                }
+        double d0, d1, d2, e0, e1, e2, f0, f1, f2;
+        iso_grad<double>([&](int p, int q, int r) { return th[0][r + 1][q + 1][p + 1]; }, d0, d1, d2);
+        iso_grad<double>([&](int p, int q, int r) { return th[1][r + 1][q + 1][p + 1]; }, e0, e1, e2);
+        iso_grad<double>([&](int p, int q, int r) { return th[2][r + 1][q + 1][p + 1]; }, f0, f1, f2);
+        divt = d0 + e1 + f2;
+        phi = PHI(x, y, z);
+        // 6 (sum_l w_l phi(x + c_l) - phi), D3Q27 weights
+        double sw = 0;
+#pragma unroll 1
+        for (int l = 0; l < 27; ++l) sw += WL<27>(l) * PHI(x + EX(l), y + EY(l), z + EZ(l));
+        lap = 6.0 * (sw - phi);
+    }
+    // moments prologue (lb_cuda_moments_module.f90:104-339)
+    double rhophi = 1.0, fxv = a.fx, fyv = a.fy, fzv = a.fz, grx = 0, gry = 0, grz = 0, mask = 0, visc = 0;
+    if (a.tc) mask = 4.0 * phi * (1.0 - phi);
+    if (a.dr) {
+        rhophi = a.rho_r * phi + (1.0 - phi) * a.rho_b;
+        fxv = rhophi * a.fx; fyv = rhophi * a.fy; fzv = rhophi * a.fz;
+    }
+    if (a.tc) {
+        const double chem = 4.0 * a.beta * phi * (phi - 1.0) * (phi - 0.5) - a.kapp * lap;
+        fxv += chem * gfx; fyv += chem * gfy; fzv += chem * gfz;
+    }
+    if (a.dr) {
+        grx = (a.rho_r - a.rho_b) * gfx; gry = (a.rho_r - a.rho_b) * gfy; grz = (a.rho_r - a.rho_b) * gfz;
+        fxv -= mask * P * cssq * grx; fyv -= mask * P * cssq * gry; fzv -= mask * P * cssq * grz;
+        const S* uin = static_cast<const S*>(a.uin);
+        const double uo = (double)CD::ld(uin, g, 1.0 / a.scale[F_UOLD]);
+        const double vo = (double)CD::ld(uin + N, g, 1.0 / a.scale[F_UOLD + 1]);
+        const double wo = (double)CD::ld(uin + 2 * N, g, 1.0 / a.scale[F_UOLD + 2]);
+        const double qxx = pi[0] - uo * uo, qyy = pi[1] - vo * vo, qzz = pi[2] - wo * wo;
+        const double qxy = pi[3] - uo * vo, qxz = pi[4] - uo * wo, qyz = pi[5] - vo * wo;
+        visc = (a.rho_r * a.visc1 * phi + (1.0 - phi) * a.visc2 * a.rho_b) / rhophi;
+        const double cv = visc / ((visc * 3.0 + 0.5) * cssq);
+        fxv -= mask * cv * (qxx * grx + qxy * gry + qxz * grz);
+        fyv -= mask * cv * (qyy * gry + qxy * grx + qyz * grz);
+        fzv -= mask * cv * (qzz * grz + qxz * grx + qyz * gry);
+        u += 0.5 * fxv / rhophi; v += 0.5 * fyv / rhophi; w += 0.5 * fzv / rhophi;
+        const double dd = (a.rho_r - a.rho_b) * (a.tau_diff * lap - a.sharp_c * divt);
+        const double den = 1.0 - 0.5 * dd / rhophi;
+        u /= den; v /= den; w /= den;
+        fxv -= dd * u; fyv -= dd * v; fzv -= dd * w;
+    } else {
+        u += 0.5 * fxv / rhophi; v += 0.5 * fyv / rhophi; w += 0.5 * fzv / rhophi;
+    }
+    m[0] = P; m[1] = u; m[2] = v; m[3] = w;
+    m[4] = pi[0] + fxv * u / rhophi;
+    m[5] = pi[1] + fyv * v / rhophi;
+    m[6] = pi[2] + fzv * w / rhophi;
+    m[7] = pi[3] + 0.5 * (fyv * u + fxv * v) / rhophi;
+    m[8] = pi[4] + 0.5 * (fzv * u + fxv * w) / rhophi;
+    m[9] = pi[5] + 0.5 * (fzv * v + fyv * w) / rhophi;
+    phi_c = phi;
+}
+
+// One thread per face node.  FP64 arithmetic, as the reference's boundary
+// code (real(kind=db)), on every storage type.
+template <typename S, int LAT, bool HO>
+__global__ void open_face_kernel(const OpenFaceArgs a) {
+    using R = typename std::conditional<sizeof(S) == 8, double, float>::type;
+    using CD = Codec<S>;
+    const int n[3] = {a.nx, a.ny, a.nz};
+    const int a1 = a.axis == 0 ? 1 : 0, a2 = a.axis == 2 ? 1 : 2;
+    const int m1 = n[a1] - 2, m2 = n[a2] - 2;
+    if (m1 <= 0 || m2 <= 0) return;
+    const long long tot = (long long)m1 * m2;
+    const long long plane = (long long)a.nx * a.ny, N = plane * a.nz;
+    const double cssq = 1.0 / 3.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        int x[3];
+        x[a.axis] = a.side ? n[a.axis] - 2 : 1;
+        x[a1] = 1 + (int)(t % m1);
+        x[a2] = 1 + (int)(t / m1);
+        const long long g = x[2] * plane + (long long)x[1] * a.nx + x[0];
+        if (a.isf[g] != -1) continue;
+        double mm[10], phi = 0;
+        face_node_moments<S>(a, x[0], x[1], x[2], g, mm, phi);
+        // Pi' = Pi - cs^2 P - u u of the node's moments after the force half-step
+        const double press = mm[0], u = mm[1], v = mm[2], w = mm[3];
+        const double pxx = mm[4] - cssq * press - u * u, pyy = mm[5] - cssq * press - v * v;
+        const double pzz = mm[6] - cssq * press - w * w;
+        const double pxy = mm[7] - u * v, pxz = mm[8] - u * w, pyz = mm[9] - v * w;
+        double om = a.omega;
+        if (a.tc) {
+            const double rhophi = a.dr ? a.rho_r * phi + (1.0 - phi) * a.rho_b : 1.0;
+            const double visc = (a.rho_r * a.visc1 * phi + (1.0 - phi) * a.visc2 * a.rho_b) / rhophi;
+            om = 1.0 / (visc * 3.0 + 0.5);
+        }
+        const double om1 = 1.0 - om;
+        double pb = press, ub = u, vb = v, wb = w;
+        if (a.type == 1) {
+            pb = a.press;
+        } else if (a.type != 2) {
+            ub = a.vel[0]; vb = a.vel[1]; wb = a.vel[2];
+        }
+        const double uu = 0.5 * (ub * ub + vb * vb + wb * wb) * 3.0;
+        // HIGHORDER coefficients of the face population (rows 10..26):
+        // equilibrium monomial + (1 - omega) x non-equilibrium projection
+        double hm[17];
+        if constexpr (HO) {
+            const double U = ub, V = vb, W = wb;
+            const double eq[17] = {U * U * V, U * U * W, U * V * V, U * W * W, V * W * W, V * V * W, U * V * W,
+                                   U * U * V * V, U * U * W * W, V * V * W * W, U * V * W * W, U * V * V * W,
+                                   U * U * V * W, U * U * V * W * W, U * U * V * V * W, U * V * V * W * W,
+                                   U * U * V * V * W * W};
+            const double nq[17] = {
+                2 * pxy * U + pxx * V,
+                2 * pxz * U + pxx * W,
+                pyy * U + 2 * pxy * V,
+                pzz * U + 2 * pxz * W,
+                pzz * V + 2 * pyz * W,
+                2 * pyz * V + pyy * W,
+                pyz * U + pxz * V + pxy * W,
+                pyy * U * U + 2 * V * (3 * pxy * U + pxx * V),
+                pzz * U * U + 2 * W * (3 * pxz * U + pxx * W),
+                pzz * V * V + 2 * W * (3 * pyz * V + pyy * W),
+                pzz * U * V + W * (3 * pyz * U + 3 * pxz * V + 2 * pxy * W),
+                2 * pyz * U * V + pxz * V * V + 2 * pyy * U * W + 4 * pxy * V * W,
+                pyz * U * U + 2 * pxz * U * V + 4 * pxy * U * W + 2 * pxx * V * W,
+                pzz * U * U * V + 3 * W * (pyz * U * U + 2 * pxz * U * V + 2 * pxy * U * W + pxx * V * W),
+                2 * U * V * (pyz * U + pxz * V) + 2 * pyy * U * U * W + V * (10 * pxy * U + 3 * pxx * V) * W,
+                pzz * U * V * V + 3 * W * (2 * pyz * U * V + pxz * V * V + pyy * U * W + 2 * pxy * V * W),
+                pzz * U * U * V * V +
+                    W * (6 * U * V * (pyz * U + pxz * V) + 3 * pyy * U * U * W + 2 * V * (7 * pxy * U + 2 * pxx * V) * W)};
+#pragma unroll
+            for (int r = 0; r < 17; ++r) hm[r] = eq[r] + om1 * nq[r];
+        }
+        // the step's output moments at the node, in the reference's convention
+        // (Pi = sum f (c c - cs^2 delta))
+        S* mom = static_cast<S*>(a.mom);
+        double o[10];
+        if constexpr (CD::scaled) o[0] = a.pres[g];
+        else o[0] = (double)CD::ld(mom, g, 1.0);
+#pragma unroll
+        for (int f = 1; f < 10; ++f) o[f] = (double)CD::ld(mom + f * N, g, 1.0 / a.scale[f]);
+        if constexpr (CD::scaled) {
+            // 16-bit storage keeps Pi - u u
+            o[4] += o[1] * o[1]; o[5] += o[2] * o[2]; o[6] += o[3] * o[3];
+            o[7] += o[1] * o[2]; o[8] += o[1] * o[3]; o[9] += o[2] * o[3];
+        }
+#pragma unroll
+        for (int l = 1; l < 27; ++l) {
+            if (!IN<LAT>(l)) continue;
+            const int cx = EX(l), cy = EY(l), cz = EZ(l);
+            // upstream node x - c_l: inside the box (the face nodes keep one
+            // node away from every box face)
+            const long long gu = g - ((long long)cz * plane + (long long)cy * a.nx + cx);
+            if (a.isf[gu] != 0) continue;
+            const double wl = WL<LAT>(l);
+            const double dx = cx, dy = cy, dz = cz;
+            const double qn = 4.5 * ((dx * dx - cssq) * pxx + (dy * dy - cssq) * pyy + (dz * dz - cssq) * pzz +
+                                     2.0 * (dx * dy) * pxy + 2.0 * (dx * dz) * pxz + 2.0 * (dy * dz) * pyz);
+            // the bounce-back population, taken out with the weights c_a c_b
+            const double fo = wl * press + om1 * (wl * qn);
+            o[0] -= fo;
+            o[1] -= fo * dx; o[2] -= fo * dy; o[3] -= fo * dz;
+            o[4] -= fo * (dx * dx); o[5] -= fo * (dy * dy); o[6] -= fo * (dz * dz);
+            o[7] -= fo * (dx * dy); o[8] -= fo * (dx * dz); o[9] -= fo * (dy * dz);
+            // the face's population
+            const double udotc = (ub * dx + vb * dy + wb * dz) * 3.0;
+            double fn = wl * (pb + udotc + 0.5 * udotc * udotc - uu) + om1 * (wl * qn);
+            if constexpr (HO) {
+                double hs = 0.0;
+#pragma unroll
+                for (int r = 0; r < 17; ++r)
+                    hs += hfac(c_hmul[r][0], cx) * hfac(c_hmul[r][1], cy) * hfac(c_hmul[r][2], cz) * hm[r];
+                fn += wl * hs;
+            }
+            o[0] += fn;
+            o[1] += fn * dx; o[2] += fn * dy; o[3] += fn * dz;
+            o[4] += fn * (dx * dx - cssq); o[5] += fn * (dy * dy - cssq); o[6] += fn * (dz * dz - cssq);
+            o[7] += fn * (dx * dy); o[8] += fn * (dx * dz); o[9] += fn * (dy * dz);
+        }
+        if constexpr (CD::scaled) {
+            a.pres[g] = (float)o[0];
+            o[4] -= o[1] * o[1]; o[5] -= o[2] * o[2]; o[6] -= o[3] * o[3];
+            o[7] -= o[1] * o[2]; o[8] -= o[1] * o[3]; o[9] -= o[2] * o[3];
+        } else {
+            CD::st(mom, g, (R)o[0], R(1));
+        }
+#pragma unroll
+        for (int f = 1; f < 10; ++f) CD::st(mom + f * N, g, (R)o[f], (R)a.scale[f]);
+    }
+}
+
+template <typename S>
+__global__ void phi_flux_kernel(int nx, int ny, int nz, int axis, int side, const S* mom, const void* phi_,
+                                const int8_t* isf, double inv_scale, double* out) {
+    using SP = typename PhiStore<S>::type;
+    using CD = Codec<S>;
+    const SP* phi = static_cast<const SP*>(phi_);
+    const int n[3] = {nx, ny, nz};
+    const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+    const long long tot = (long long)n[a1] * n[a2];
+    const long long plane = (long long)nx * ny, N = plane * nz;
+    const S* un = mom + (1 + axis) * N;
+    double acc = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        int x[3];
+        x[axis] = side ? n[axis] - 2 : 1;
+        x[a1] = (int)(t % n[a1]);
+        x[a2] = (int)(t / n[a1]);
+        const long long g = x[2] * plane + (long long)x[1] * nx + x[0];
+        if (isf[g] != -1) continue;
+        const double q = (double)CD::ld(un, g, inv_scale) * (double)phi[g];
+        acc += side ? -q : q;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, red[0]);
+}
+
+}  // namespace
+
+cudaError_t launch_open_face(int storage, const OpenFaceArgs& a, cudaStream_t st) {
+    const int n[3] = {a.nx, a.ny, a.nz};
+    const long long tot = (long long)(n[a.axis == 0 ? 1 : 0] - 2) * (n[a.axis == 2 ? 1 : 2] - 2);
+    if (tot <= 0 || n[a.axis] < 3) return cudaSuccess;
+    const int grid = grid_for(tot, 128);
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        if (a.lattice == 27 && a.highorder) open_face_kernel<S, 27, true><<<grid, 128, 0, st>>>(a);
+        else if (a.lattice == 27) open_face_kernel<S, 27, false><<<grid, 128, 0, st>>>(a);
+        else if (a.lattice == 19) open_face_kernel<S, 19, false><<<grid, 128, 0, st>>>(a);
+        else open_face_kernel<S, 15, false><<<grid, 128, 0, st>>>(a);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const void* phi,
+                            const int8_t* isf, const double* inv_scale, double* d_flux, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_flux, 0, sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    const int n[3] = {nx, ny, nz};
+    return by_storage(storage, [&](auto tag) {
+        using S = decltype(tag);
+        for (int axis = 0; axis < 3; ++axis) {
+            if (!(open & (1 << axis)) || n[axis] < 3) continue;
+            const long long tot = (long long)n[axis == 0 ? 1 : 0] * n[axis == 2 ? 1 : 2];
+            for (int side = 0; side < 2; ++side)
+                phi_flux_kernel<S><<<grid_for(tot, 256), 256, 0, st>>>(nx, ny, nz, axis, side,
+                                                                       static_cast<const S*>(mom), phi, isf,
+                                                                       inv_scale[1 + axis], d_flux);
+        }
+        return cudaGetLastError();
+    });
+}
+
+}  // namespace lbf

@@ -26,6 +26,7 @@
  *   fused collide+stream  lb_cuda_fused_module.f90:426-750
  *   update_phi            lb_cuda_update_phi_module.f90:19-104
  *   obstacle bounce-back  lb_cuda_boundary_module.f90:19-216
+ *   open boundaries       boundary_cds_module.f90:57-1311 (moments), 1351-1663 (phi), 1667-1885 (flux)
  *   copy_print            print_module.f90:638-776
  *   lattice tables        vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15)
  *   parameter derivation  LBFAST.f90:212-219
@@ -77,6 +78,14 @@ typedef struct orc_params {
     double wettab_r;
     int phi_correction; /* phi mass correction after every step (see mass_correction) */
     int smagorinsky;    /* SMAGORINSKI LES relaxation time (see smag_omega) */
+    /* open boundaries (openbc = 1, INTERNAL_OBSTACLES): per axis x, y, z and
+     * side (low, high) the openbc_type_x/y/z, openbc_press_x/y/z and
+     * (openbc_u, openbc_v, openbc_w)_x/y/z values of the input file
+     * (vars_module.f90:238-255); see open_face */
+    int openbc;
+    int obc_type[3][2];
+    double obc_press[3][2];
+    double obc_vel[3][2][3];
 } orc_params;
 
 /* ---- lattice tables: vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15) ---- */
@@ -836,6 +845,192 @@ static void obstacle_bb(orc_state *s, real **hin, real **hout, const real *ph)
     }
 }
 
+/* Open face (axis 0/1/2 = x/y/z, side 0 = low, 1 = high) of
+ * bcs_mesoscopic_hfields, boundary_cds_module.f90:57-1311, run after
+ * LB_int_boundary on the moments B of the step.  Nodes: isfluid = -1 on the
+ * plane next to the wall (reference gi = 2 or lx-1), the two tangential
+ * indices strictly inside (1, l) of the reference's 1-based range.  For every
+ * link l whose upstream node x - c_l is a wall (isfluid = 0) the population
+ * w_l P + (1 - omega) fneq(Pi') is taken out of B with the weights c_a c_b,
+ * and the population of the face's state is added with c_a c_b - cs^2 delta
+ * (HIGHORDER: with the Minv_mrt rows 10-26 of the face velocity), where
+ * Pi' = Pi - cs^2 P - u u from the node's moments after the force half-step
+ * (A), and omega is the molecular relaxation rate of the node's phi.  Face
+ * types (openbc_type): 2 zero gradient (the node's P and u), 1 pressure
+ * (openbc_press, the node's u), other velocity (the node's P, openbc_u/v/w).
+ * The removal does not invert the bounce-back (other Pi, other weights):
+ * both are kept as the reference writes them. */
+static void open_face(orc_state *s, real **hin, real **hout, const real *ph, int axis, int side)
+{
+    const int tc = s->p.twocomp, dr = s->p.densratio, ho = s->p.highorder && s->p.lattice == 27;
+    const real cssq = (real)(1.0 / 3.0), invcssq = (real)3.0, ONE = (real)1.0, HALF = (real)0.5, TWO = (real)2.0;
+    const real THREE = (real)3.0, FOUR = (real)4.0, SIX = (real)6.0, SEVEN = (real)7.0, TEN = (real)10.0;
+    const int n[3] = {s->nx, s->ny, s->nz};
+    const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;  /* tangential axes */
+    const int plane = side ? n[axis] - 2 : 1;
+    const int type = s->p.obc_type[axis][side];
+    int t2;
+#pragma omp parallel for schedule(static)
+    for (t2 = 1; t2 <= n[a2] - 2; t2++) {
+        int t1, l, r;
+        for (t1 = 1; t1 <= n[a1] - 2; t1++) {
+            int x[3];
+            x[axis] = plane; x[a1] = t1; x[a2] = t2;
+            const int i = x[0], j = x[1], k = x[2];
+            long c = IDX(s, i, j, k);
+            if (s->isf[c] != -1) continue;
+            real press = hin[0][c], u = hin[1][c], v = hin[2][c], w = hin[3][c];
+            real pxx = hin[4][c], pyy = hin[5][c], pzz = hin[6][c];
+            real pxy = hin[7][c], pxz = hin[8][c], pyz = hin[9][c];
+            real o[10];
+            for (l = 0; l < 10; l++) o[l] = hout[l][c];
+            real presstmp = press, utmp = u, vtmp = v, wtmp = w;
+            if (type == 1) {
+                presstmp = (real)s->p.obc_press[axis][side];
+            } else if (type != 2) {
+                utmp = (real)s->p.obc_vel[axis][side][0];
+                vtmp = (real)s->p.obc_vel[axis][side][1];
+                wtmp = (real)s->p.obc_vel[axis][side][2];
+            }
+            pxx = pxx - cssq * press - u * u;
+            pyy = pyy - cssq * press - v * v;
+            pzz = pzz - cssq * press - w * w;
+            pxy = pxy - u * v;
+            pxz = pxz - u * w;
+            pyz = pyz - v * w;
+            real om = s->omega;
+            if (tc) {
+                real phi = ph[c], rhophi = ONE;
+                if (dr) rhophi = s->rho_r * phi + (ONE - phi) * s->rho_b;
+                real visc = (s->rho_r * s->visc1 * phi + (ONE - phi) * s->visc2 * s->rho_b) / rhophi;
+                om = ONE / (visc * invcssq + HALF);
+            }
+            real uu = HALF * (utmp * utmp + vtmp * vtmp + wtmp * wtmp) * invcssq;
+            /* HIGHORDER terms of the face population (rows 10..26): equilibrium
+             * monomials and non-equilibrium projections */
+            real meq[27], mneq[27];
+            if (ho) {
+                const real U = utmp, V = vtmp, W = wtmp;
+                meq[10] = U * U * V; meq[11] = U * U * W; meq[12] = U * V * V; meq[13] = U * W * W;
+                meq[14] = V * W * W; meq[15] = V * V * W; meq[16] = U * V * W;
+                meq[17] = U * U * V * V; meq[18] = U * U * W * W; meq[19] = V * V * W * W;
+                meq[20] = U * V * W * W; meq[21] = U * V * V * W; meq[22] = U * U * V * W;
+                meq[23] = U * U * V * W * W; meq[24] = U * U * V * V * W; meq[25] = U * V * V * W * W;
+                meq[26] = U * U * V * V * W * W;
+                mneq[10] = TWO * pxy * U + pxx * V;
+                mneq[11] = TWO * pxz * U + pxx * W;
+                mneq[12] = pyy * U + TWO * pxy * V;
+                mneq[13] = pzz * U + TWO * pxz * W;
+                mneq[14] = pzz * V + TWO * pyz * W;
+                mneq[15] = TWO * pyz * V + pyy * W;
+                mneq[16] = pyz * U + pxz * V + pxy * W;
+                mneq[17] = pyy * U * U + TWO * V * (THREE * pxy * U + pxx * V);
+                mneq[18] = pzz * U * U + TWO * W * (THREE * pxz * U + pxx * W);
+                mneq[19] = pzz * V * V + TWO * W * (THREE * pyz * V + pyy * W);
+                mneq[20] = pzz * U * V + W * (THREE * pyz * U + THREE * pxz * V + TWO * pxy * W);
+                mneq[21] = TWO * pyz * U * V + pxz * V * V + TWO * pyy * U * W + FOUR * pxy * V * W;
+                mneq[22] = pyz * U * U + TWO * pxz * U * V + FOUR * pxy * U * W + TWO * pxx * V * W;
+                mneq[23] = pzz * U * U * V + THREE * W * (pyz * U * U + TWO * pxz * U * V + TWO * pxy * U * W + pxx * V * W);
+                mneq[24] = TWO * U * V * (pyz * U + pxz * V) + TWO * pyy * U * U * W + V * (TEN * pxy * U + THREE * pxx * V) * W;
+                mneq[25] = pzz * U * V * V + THREE * W * (TWO * pyz * U * V + pxz * V * V + pyy * U * W + TWO * pxy * V * W);
+                mneq[26] = pzz * U * U * V * V +
+                           W * (SIX * U * V * (pyz * U + pxz * V) + THREE * pyy * U * U * W + TWO * V * (SEVEN * pxy * U + TWO * pxx * V) * W);
+            }
+            for (l = 1; l < s->nl; l++) {
+                int lo = s->opp[l];
+                if (s->isf[IDX(s, i + s->ex[lo], j + s->ey[lo], k + s->ez[lo])] != 0) continue;
+                real dex = (real)s->ex[l], dey = (real)s->ey[l], dez = (real)s->ez[l];
+                real feq = s->w[l] * press;
+                real fneq = s->w[l] * (HALF / (cssq * cssq)) *
+                            ((dex * dex - cssq) * pxx + (dey * dey - cssq) * pyy + (dez * dez - cssq) * pzz +
+                             TWO * (dex * dey) * pxy + TWO * (dex * dez) * pxz + TWO * (dey * dez) * pyz);
+                real fp = feq + (ONE - om) * fneq;
+                o[0] = o[0] - fp;
+                o[1] = o[1] - fp * dex; o[2] = o[2] - fp * dey; o[3] = o[3] - fp * dez;
+                o[4] = o[4] - fp * dex * dex; o[5] = o[5] - fp * dey * dey; o[6] = o[6] - fp * dez * dez;
+                o[7] = o[7] - fp * dex * dey; o[8] = o[8] - fp * dex * dez; o[9] = o[9] - fp * dey * dez;
+                real udotc = (utmp * dex + vtmp * dey + wtmp * dez) * invcssq;
+                feq = s->w[l] * (presstmp + udotc + HALF * udotc * udotc - uu);
+                if (ho)
+                    for (r = 10; r < 27; r++) {
+                        feq = feq + s->minv[r][l] * meq[r];
+                        fneq = fneq + s->minv[r][l] * mneq[r];
+                    }
+                fp = feq + (ONE - om) * fneq;
+                o[0] = o[0] + fp;
+                o[1] = o[1] + fp * dex; o[2] = o[2] + fp * dey; o[3] = o[3] + fp * dez;
+                o[4] = o[4] + fp * (dex * dex - cssq);
+                o[5] = o[5] + fp * (dey * dey - cssq);
+                o[6] = o[6] + fp * (dez * dez - cssq);
+                o[7] = o[7] + fp * dex * dey; o[8] = o[8] + fp * dex * dez; o[9] = o[9] + fp * dey * dez;
+            }
+            for (l = 0; l < 10; l++) hout[l][c] = o[l];
+        }
+    }
+}
+
+/* the open faces in the reference's order: x low, x high, y low, ..., on
+ * the non-periodic axes */
+static void open_bc(orc_state *s, real **hin, real **hout, const real *ph)
+{
+    const int pbc[3] = {s->p.pbc_x, s->p.pbc_y, s->p.pbc_z};
+    int axis, side;
+    for (axis = 0; axis < 3; axis++)
+        if (!pbc[axis])
+            for (side = 0; side < 2; side++) open_face(s, hin, hout, ph, axis, side);
+}
+
+/* Open boundaries, phase field (bcs_mesoscopic_phifields after
+ * PHI_int_boundary, boundary_cds_module.f90:1351-1663): on each open face the
+ * wall nodes (reference gi = 1 or lx), tangential indices strictly inside
+ * (1, l), take the phi of their neighbour on the plane next to them. */
+static void open_phi_copy(orc_state *s, real *ph)
+{
+    const int pbc[3] = {s->p.pbc_x, s->p.pbc_y, s->p.pbc_z};
+    const int n[3] = {s->nx, s->ny, s->nz};
+    int axis, side, t1, t2;
+    for (axis = 0; axis < 3; axis++) {
+        if (pbc[axis]) continue;
+        const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+        for (side = 0; side < 2; side++)
+            for (t2 = 1; t2 <= n[a2] - 2; t2++)
+                for (t1 = 1; t1 <= n[a1] - 2; t1++) {
+                    int x[3], y[3];
+                    x[axis] = side ? n[axis] - 1 : 0; x[a1] = t1; x[a2] = t2;
+                    y[axis] = side ? n[axis] - 2 : 1; y[a1] = t1; y[a2] = t2;
+                    ph[IDX(s, x[0], x[1], x[2])] = ph[IDX(s, y[0], y[1], y[2])];
+                }
+    }
+}
+
+/* Phi carried through the open faces in one step (BCPHIFLUX,
+ * boundary_cds_module.f90:1667-1861): over the isfluid = -1 nodes of the
+ * planes next to the walls (no tangential limits), + u_n phi on low faces and
+ * - u_n phi on high faces, u_n the moment velocity normal to the face, in
+ * FP64. */
+static double phi_flux(const orc_state *s, real **h, const real *ph)
+{
+    const int pbc[3] = {s->p.pbc_x, s->p.pbc_y, s->p.pbc_z};
+    const int n[3] = {s->nx, s->ny, s->nz};
+    double flux = 0.0;
+    int axis, side, t1, t2;
+    for (axis = 0; axis < 3; axis++) {
+        if (pbc[axis]) continue;
+        const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+        for (side = 0; side < 2; side++)
+            for (t2 = 0; t2 < n[a2]; t2++)
+                for (t1 = 0; t1 < n[a1]; t1++) {
+                    int x[3];
+                    x[axis] = side ? n[axis] - 2 : 1; x[a1] = t1; x[a2] = t2;
+                    long c = IDX(s, x[0], x[1], x[2]);
+                    if (s->isf[c] != -1) continue;
+                    double q = (double)h[1 + axis][c] * (double)ph[c];
+                    flux += side ? -q : q;
+                }
+    }
+    return flux;
+}
+
 /* copy_print: print_module.f90:638-776 (stepskip = 1) */
 static void copy_print(orc_state *s, real **hs, const real *ph)
 {
@@ -891,16 +1086,19 @@ static double phi_sum_count(const orc_state *s, const real *ph, long *cnt)
  * apply_lagrangian_phi_kernel, lb_cuda_boundary_module.f90:509-563): the
  * lost mass dphi = sum0 - sum is spread over the interface nodes,
  * corr = dphi / count added to every fluid node with 0.5 < phi < 0.9.  The
- * reference applies it only with open boundaries, where sum0 is corrected by
- * the boundary fluxes; with periodic and wall boundaries those are zero.
- * Applied here to the new phi of every step. */
-static void mass_correction(orc_state *s, real *ph)
+ * reference applies it only with open boundaries, where the target is
+ * sum0 + flux, flux the phi carried through the open faces (phi_flux) by the
+ * step's moments; with periodic and wall boundaries it is zero.  The
+ * reference corrects the input phi of a step after compute_norm; here the
+ * output phi of every step is corrected, with the flux of the output moments
+ * and phi -- the same quantities one call earlier. */
+static void mass_correction(orc_state *s, real *ph, double flux)
 {
     long cnt = 0;
     double sum = phi_sum_count(s, ph, &cnt), corr;
     int i, j, k;
     if (cnt == 0) return;
-    corr = (s->phi_sum0 - sum) / (double)cnt;
+    corr = (s->phi_sum0 + flux - sum) / (double)cnt;
     for (k = 0; k < s->nz; k++)
         for (j = 0; j < s->ny; j++)
             for (i = 0; i < s->nx; i++) {
@@ -917,7 +1115,15 @@ static void prime(orc_state *s)
 {
     real **A = s->h[s->flip];
     if (s->p.twocomp) s->phi_sum0 = phi_sum_count(s, s->phi[s->flip], NULL);
-    if (s->p.twocomp && s->p.obstacles) wetting(s, s->phi[s->flip]);
+    if (s->p.twocomp && s->p.obstacles) {
+        wetting(s, s->phi[s->flip]);
+        if (s->p.openbc) {
+            open_phi_copy(s, s->phi[s->flip]);
+            /* the pre-loop bcs_mesoscopic_phifields corrects once with the
+             * flux of the initial state (integrator_module.f90:179-182) */
+            if (s->p.phi_correction) mass_correction(s, s->phi[s->flip], phi_flux(s, A, s->phi[s->flip]));
+        }
+    }
     copy_print(s, A, s->phi[s->flip]);
     if (s->p.twocomp) halo_real(s, s->phi[s->flip]);
     exchange_h(s, A);
@@ -933,7 +1139,10 @@ static void one_step(orc_state *s)
     if (s->p.twocomp) {
         compute_norm(s, pA);
         for (f = 0; f < 7; f++) halo_real(s, s->aux[f]);
-        if (s->p.obstacles) wetting(s, pA);
+        if (s->p.obstacles) {
+            wetting(s, pA);
+            if (s->p.openbc) open_phi_copy(s, pA);
+        }
         compute_div_theta(s);
     }
     moments(s, A, B, pA);
@@ -941,12 +1150,16 @@ static void one_step(orc_state *s)
     for (f = 0; f < 3; f++) halo_real(s, s->frc[f]);
     copy_print(s, A, pA);
     fused(s, A, B, pA);
+    if (s->p.twocomp) update_phi(s, A, pA, pB);
+    if (s->p.obstacles) {
+        obstacle_bb(s, A, B, pA);
+        if (s->p.openbc) open_bc(s, A, B, pA);
+    }
     if (s->p.twocomp) {
-        update_phi(s, A, pA, pB);
-        if (s->p.phi_correction) mass_correction(s, pB);
+        if (s->p.phi_correction)
+            mass_correction(s, pB, s->p.obstacles && s->p.openbc ? phi_flux(s, B, pB) : 0.0);
         halo_real(s, pB);
     }
-    if (s->p.obstacles) obstacle_bb(s, A, B, pA);
     s->flip = out;
     s->step++;
 }

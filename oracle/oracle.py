@@ -32,6 +32,8 @@ class OrcParams(C.Structure):
         ("rho_b", C.c_double), ("sigma", C.c_double), ("width", C.c_double),
         ("tau_diff", C.c_double), ("fx", C.c_double), ("fy", C.c_double),
         ("fz", C.c_double), ("wettab_r", C.c_double), ("phi_correction", C.c_int), ("smagorinsky", C.c_int),
+        ("openbc", C.c_int), ("obc_type", (C.c_int * 2) * 3), ("obc_press", (C.c_double * 2) * 3),
+        ("obc_vel", ((C.c_double * 3) * 2) * 3),
     ]
 
 
@@ -101,7 +103,8 @@ def set_threads(n: int) -> None:
 
 PARAM_KEYS = ("lx", "ly", "lz", "pbc_x", "pbc_y", "pbc_z", "lattice", "highorder",
               "twocomp", "densratio", "obstacles", "visc1", "visc2", "rho_r", "rho_b",
-              "sigma", "width", "tau_diff", "fx", "fy", "fz", "wettab_r", "phi_correction", "smagorinsky")
+              "sigma", "width", "tau_diff", "fx", "fy", "fz", "wettab_r", "phi_correction", "smagorinsky",
+              "openbc")
 
 
 class Oracle:
@@ -114,6 +117,16 @@ class Oracle:
         p = OrcParams()
         for k in PARAM_KEYS:
             setattr(p, k, params.get(k, 0) if k not in ("rho_r", "rho_b") else params.get(k, 1.0))
+        # open faces: openbc_type / openbc_press [axis][side], openbc_vel [axis][side][u, v, w]
+        ty = params.get("openbc_type") or ((0, 0),) * 3
+        pr = params.get("openbc_press") or ((0.0, 0.0),) * 3
+        ve = params.get("openbc_vel") or (((0.0,) * 3,) * 2,) * 3
+        for a in range(3):
+            for sd in range(2):
+                p.obc_type[a][sd] = int(ty[a][sd])
+                p.obc_press[a][sd] = float(pr[a][sd])
+                for d in range(3):
+                    p.obc_vel[a][sd][d] = float(ve[a][sd][d])
         self.p = dict(params)
         self.shape = (int(params["lz"]), int(params["ly"]), int(params["lx"]))
         self.n = int(np.prod(self.shape))

@@ -113,6 +113,60 @@ def make_case(name: str, storage: str = "f32"):
         m = np.where((isf == 0)[None], 0.0, m)
         m = np.nan_to_num(m)
         return p, isf, m, phi
+    if name in ("open_q27ho_2c_dr", "open_q27_2c", "open_q15_2c_dr"):
+        # open faces (openbc = 1) on every non-periodic axis, all three face
+        # types, nodes next to two and three faces at the box edges and
+        # corners.  Pressure and zero-gradient faces sit on one axis only:
+        # the edge nodes get the replacements of both faces, which do not
+        # invert the bounce-back, and where a pressure or zero-gradient axis
+        # meets another such axis or a moving velocity face the run diverges
+        # within tens to hundreds of steps (the reference's loops as written);
+        # resting velocity faces on the other axes.
+        lat = 15 if "q15" in name else 27
+        ho = 1 if "ho" in name else 0
+        dr = 1 if name.endswith("dr") else 0
+        if name == "open_q27ho_2c_dr":
+            L, pbc = (30, 18, 14), (0, 0, 0)
+            ty = ((1, 2), (0, 0), (0, 0))
+            pr = ((0.001, 0.0), (0.0, 0.0), (0.0, 0.0))
+            ve = (((0.0,) * 3,) * 2,) * 3
+        elif name == "open_q27_2c":
+            L, pbc = (28, 16, 12), (0, 1, 1)
+            ty = ((0, 2), (0, 0), (0, 0))
+            pr = ((0.0, 0.0),) * 3
+            ve = (((0.005, 0.0, 0.0), (0.0,) * 3), ((0.0,) * 3,) * 2, ((0.0,) * 3,) * 2)
+        else:
+            L, pbc = (20, 16, 26), (1, 1, 0)
+            ty = ((0, 0), (0, 0), (1, 0))
+            pr = ((0.0, 0.0), (0.0, 0.0), (0.002, 0.0))
+            ve = (((0.0,) * 3,) * 2, ((0.0,) * 3,) * 2, ((0.0,) * 3, (0.0, 0.0, -0.003)))
+        p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_x=pbc[0], pbc_y=pbc[1], pbc_z=pbc[2], lattice=lat, highorder=ho,
+                   twocomponent=1, densratio=dr, obstacles=1, visc1=0.05, visc2=0.1, rho_r=1.0,
+                   rho_b=0.25 if dr else 1.0, sigma=0.01, width=4.0, tau_diff=0.1, fx=2e-6, wettab_r=75.0,
+                   storage=storage, openbc=1, openbc_type=ty, openbc_press=pr, openbc_vel=ve)
+        solid = np.zeros(p.shape, dtype=bool)
+        if lat == 27:
+            solid |= _spheres_solid(rng, p.shape, 2, 2.0, 3.0)
+        else:
+            solid[10:15, 5:10, 6:11] = True  # no corner-only solid nodes (see above)
+        isf = O.mark_isfluid(solid, pbc, lat, True)
+        phi = _blobs(rng, p.shape, 4, 2.5, 5.0, 4.0)
+        phi = np.where(isf == 0, 0.0, phi)
+        phi = O.seed_solid_phi(phi, isf, lat)
+        m = _random_moments(rng, p.shape, amp_u=0.003, amp_p=0.002, amp_neq=1e-5)
+        m = np.where((isf == 0)[None], 0.0, m)
+        return p, isf, np.nan_to_num(m), phi
+    if name == "open_q19_1c":
+        # pressure-driven channel: pressure faces on x, velocity-0 faces on z
+        L = (26, 10, 14)
+        p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_x=0, pbc_y=1, pbc_z=0, lattice=19, obstacles=1, visc1=0.1,
+                   storage=storage, openbc=1, openbc_type=((1, 1), (0, 0), (0, 0)),
+                   openbc_press=((0.004, -0.004), (0.0, 0.0), (0.0, 0.0)))
+        solid = _spheres_solid(rng, p.shape, 1, 2.0, 3.0)
+        isf = O.mark_isfluid(solid, (0, 1, 0), 19, True)
+        m = _random_moments(rng, p.shape, amp_u=0.003, amp_p=0.002)
+        m = np.where((isf == 0)[None], 0.0, m)
+        return p, isf, m, None
     if name == "obs_q19_1c":
         L = (28, 18, 12)
         p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_y=0, lattice=19, obstacles=1, visc1=0.1, fx=1e-5,
@@ -127,7 +181,8 @@ def make_case(name: str, storage: str = "f32"):
 
 ALL_CASES = ["tg_q19", "q27ho_1c_force", "q27_1c", "q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c",
              "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr", "q27ho_1c_force_smag",
-             "obs_q27ho_2c_dr_smag", "q19_2c_smag", "q15_1c", "q15_2c_dr", "obs_q15_2c_dr"]
+             "obs_q27ho_2c_dr_smag", "q19_2c_smag", "q15_1c", "q15_2c_dr", "obs_q15_2c_dr", "open_q27ho_2c_dr",
+             "open_q27_2c", "open_q15_2c_dr", "open_q19_1c", "open_q27ho_2c_dr_corr"]
 
 
 def run_oracle(name: str, nsteps: int, prec: str = "f64"):

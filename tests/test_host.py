@@ -97,13 +97,30 @@ def test_namelist_reader_rejects_bad_input(tmp_path):
     base = open(os.path.join(ROOT, "tests", "golden", "channel.inp")).read()
     cases = {"unknown": base.replace("lx=36", "lx=36\n   bogus_key=3"),
              "badreal": base.replace("fx=1.0d-5", "fx=1.0x-5"),
-             "openbc": base.replace("openbc=0", "openbc=1"),
+             "badelement": base.replace("openbc=0", "openbc=1\n   openbc_type_x(3)=1"),
+             "badopenkey": base.replace("openbc=0", "openbc=1\n   openbc_q_x=1"),
              "nofluid": base.split("&fluid")[0]}
     for name, text in cases.items():
         f = tmp_path / f"{name}.inp"
         f.write_text(text)
         rc, _, _ = read_nml(f)
         assert rc != 0, name
+
+
+def test_namelist_reader_reads_open_faces(tmp_path):
+    """openbc and the openbc_* arrays of vars_module.f90:238-255, whole-array
+    and element assignments, go to the parameters."""
+    base = open(os.path.join(ROOT, "tests", "golden", "channel.inp")).read()
+    text = base.replace("openbc=0", "openbc=1\n   openbc_type_x=1,2\n   openbc_press_x(1)=0.01d0\n"
+                                    "   openbc_type_y(2)=0\n   openbc_u_y(2)=0.05\n   openbc_w_z=0.5,-0.25")
+    f = tmp_path / "open.inp"
+    f.write_text(text)
+    rc, p, r = read_nml(f)
+    assert rc == 0 and p.openbc == 1 and r.openbc == 1
+    assert [list(t) for t in p.openbc_type] == [[1, 2], [0, 0], [0, 0]]
+    assert p.openbc_press[0][0] == 0.01 and p.openbc_press[0][1] == 0.0
+    assert p.openbc_vel[1][1][0] == 0.05 and list(p.openbc_vel[2][0]) == [0.0, 0.0, 0.5]
+    assert p.openbc_vel[2][1][2] == -0.25
 
 
 def test_namelist_reader_reads_reference_inputs():
@@ -134,7 +151,8 @@ def test_raw_xdmf_writer(tmp_path):
 
 
 @pytest.mark.parametrize("bad", [dict(lattice=13), dict(highorder=1, lattice=19), dict(densratio=1),
-                                 dict(lx=0), dict(storage="f8"), dict(visc1=-1.0)])
+                                 dict(lx=0), dict(storage="f8"), dict(visc1=-1.0), dict(openbc=1, pbc_x=0),
+                                 dict(openbc=1, obstacles=1, pbc_y=0, ly=2)])
 def test_create_rejects_invalid_parameters_before_device_work(bad):
     kw = dict(lx=8, ly=8, lz=8, lattice=27)
     kw.update(bad)

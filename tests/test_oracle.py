@@ -153,3 +153,50 @@ def test_lattice_tables_match_the_reference(lattice):
     assert [g27["ex"][l] for l in sub] == g["ex"]
     assert [g27["ey"][l] for l in sub] == g["ey"]
     assert [g27["ez"][l] for l in sub] == g["ez"]
+
+
+def _open_channel(types, press, vel, lx=40, ly=14, lz=4, steps=2000):
+    """Channel along x between resting velocity faces at y (walls at y = 0 and
+    ly-1), periodic in z, open x faces; one component, D3Q19."""
+    isf = O.mark_isfluid(np.zeros((lz, ly, lx), bool), (0, 0, 1), 19, True)
+    p = dict(lx=lx, ly=ly, lz=lz, pbc_x=0, pbc_y=0, pbc_z=1, lattice=19, obstacles=1, visc1=0.1, openbc=1,
+             openbc_type=(types, (0, 0), (0, 0)), openbc_press=(press, (0.0, 0.0), (0.0, 0.0)),
+             openbc_vel=(vel, ((0.0,) * 3,) * 2, ((0.0,) * 3,) * 2))
+    o = O.Oracle(p)
+    o.set_isfluid(isf)
+    o.set_fields(np.zeros((10, lz, ly, lx)))
+    o.step(steps)
+    h, _, _ = o.get_fields()
+    return h
+
+
+def test_open_pressure_faces_drive_poiseuille_flow():
+    """Pressure faces at x (boundary_cds_module.f90:57-470, openbc_type 1):
+    the steady flow is a Poiseuille profile for the interior pressure
+    gradient, u(y) = G / (2 nu) (H^2 - (y - yc)^2) with p = P / 3 and the
+    bounce-back walls on the solid rows (H = (ly - 1) / 2)."""
+    lx, ly = 40, 14
+    h = _open_channel((1, 1), (0.01, -0.01), ((0.0,) * 3,) * 2, lx=lx, ly=ly)
+    # -dp/dx from a linear fit of P along the middle of the channel (the
+    # faces distort the few planes next to them)
+    xs = np.arange(10, lx - 10)
+    G = -np.polyfit(xs, h[0, 2, ly // 2, xs], 1)[0] / 3.0
+    assert G > 0
+    y = np.arange(ly)
+    Hh, yc = (ly - 1) / 2, (ly - 1) / 2
+    theory = G / (2 * 0.1) * (Hh * Hh - (y - yc) ** 2)
+    u = h[1, 2, :, lx // 2]
+    inner = slice(1, ly - 1)
+    assert np.abs(u[inner] - theory[inner]).max() < 0.02 * theory.max()
+    assert np.abs(h[2:4, 2, inner, lx // 2]).max() < 1e-4 * theory.max()  # no cross flow
+
+
+def test_open_velocity_inlet_conserves_the_flow_rate():
+    """Velocity face at x low (openbc_type 0) and pressure face at x high: the
+    steady flow rate through every interior plane is the same and positive."""
+    lx, ly = 48, 14
+    h = _open_channel((0, 1), (0.0, 0.0), ((0.01, 0.0, 0.0), (0.0,) * 3), lx=lx, ly=ly, steps=3000)
+    q = h[1, 1, 1:ly - 1, :].sum(0)
+    inner = q[10:lx - 10]  # planes away from the faces' distortion
+    assert inner.min() > 0
+    assert (inner.max() - inner.min()) < 1e-3 * inner.mean()
