@@ -96,6 +96,10 @@ typedef struct lbf_params {
                                 value velocity (the node's P, openbc_vel) */
     double openbc_press[3][2];   /* pressure moment P of a pressure face (openbc_press_x/y/z) */
     double openbc_vel[3][2][3];  /* (u, v, w) of a velocity face (openbc_u/v/w_x/y/z) */
+    int bounce_back;         /* BOUNCE_BACK (requires obstacles): half-way bounce-back -- a link whose upstream
+                                node is solid brings the node's own post-collision population of the opposite
+                                link (fused_LB_kernel_bb, lb_cuda_fused_module.f90:20-424) -- instead of the
+                                moment-space correction of LB_int_boundary */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;

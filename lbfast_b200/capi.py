@@ -44,6 +44,7 @@ class LbfParams(C.Structure):
         ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int), ("phi_correction", C.c_int),
         ("smagorinsky", C.c_int), ("openbc", C.c_int), ("openbc_type", (C.c_int * 2) * 3),
         ("openbc_press", (C.c_double * 2) * 3), ("openbc_vel", ((C.c_double * 3) * 2) * 3),
+        ("bounce_back", C.c_int),
     ]
 
 
@@ -171,6 +172,7 @@ class Params:
     openbc_type: tuple = ((0, 0), (0, 0), (0, 0))
     openbc_press: tuple = ((0.0, 0.0), (0.0, 0.0), (0.0, 0.0))
     openbc_vel: tuple = (((0.0,) * 3,) * 2,) * 3
+    bounce_back: int = 0  # half-way bounce-back at obstacles (BOUNCE_BACK)
 
     def to_c(self) -> LbfParams:
         p = LbfParams()

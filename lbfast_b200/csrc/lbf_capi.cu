@@ -89,6 +89,7 @@ void free_all(lbf_handle* h) {
     cudaFree(h->d_err);
     cudaFree(h->d_red);
     cudaFree(h->d_mass);
+    cudaFree(h->bb_nodes);
     cudaFree(h->staging);
 }
 
@@ -319,6 +320,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (p->phi_correction && !p->twocomponent) return fail(LBF_E_ARG, "phi_correction requires TWOCOMPONENT");
     // bcs_mesoscopic_hfields / _phifields run only with INTERNAL_OBSTACLES (integrator_module.f90:514-523)
     if (p->openbc && !p->obstacles) return fail(LBF_E_ARG, "openbc requires obstacles (INTERNAL_OBSTACLES)");
+    if (p->bounce_back && !p->obstacles) return fail(LBF_E_ARG, "bounce_back requires obstacles (INTERNAL_OBSTACLES)");
     // an open axis holds a wall, the face plane and a wall at least
     if (p->openbc && ((!p->pbc_x && p->lx < 3) || (!p->pbc_y && p->ly < 3) || (!p->pbc_z && p->lz < 3)))
         return fail(LBF_E_ARG, "openbc: a non-periodic axis needs at least 3 nodes");
@@ -418,6 +420,19 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
     }
     CUDA_TRY(cudaMemcpyAsync(h->isf, isf, h->N, cudaMemcpyHostToDevice, h->stream));
     h->isf_set = true;
+    if (h->p.bounce_back) {
+        // BOUNCE_BACK: the nodes whose wall links the half-way bounce-back rewrites
+        std::vector<long long> nb;
+        for (long long i = 0; i < h->N; ++i)
+            if (isf[i] == -1) nb.push_back(i);
+        cudaFree(h->bb_nodes);
+        h->bb_nodes = nullptr;
+        h->nbb = (long long)nb.size();
+        if (h->nbb) {
+            CUDA_TRY(cudaMalloc(&h->bb_nodes, nb.size() * sizeof(long long)));
+            CUDA_TRY(cudaMemcpy(h->bb_nodes, nb.data(), nb.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        }
+    }
     if (!h->tc) return LBF_OK;
     // wetting tables: PHI_int_boundary_kernel steps 1-2 (lb_cuda_boundary_module.f90:281-398),
     // in double; they depend on isfluid only.
@@ -832,11 +847,18 @@ size_t handle_bytes(const lbf_params* p) {
 int handle_pre_step(lbf_handle* h) { return launch_wet(h, h->cur, 1 - h->cur, false); }
 
 int handle_post_step(lbf_handle* h) {
-    // open faces on the step's output moments (buffer cur after the advance),
-    // from the step's input buffers (1 - cur), which the step left intact
-    if (h->obc_open) {
+    // wall passes on the step's output moments (buffer cur after the advance),
+    // from the step's input buffers (1 - cur), which the step left intact:
+    // BOUNCE_BACK, then the open faces (bcs_mesoscopic_hfields after the fused kernel)
+    if (h->obc_open || h->nbb) {
         const int in = 1 - h->cur;
-        lbf::OpenFaceArgs a;
+        lbf::BoundaryArgs a;
+        a.smag = h->p.smagorinsky;
+        a.nodes = h->bb_nodes;
+        a.nnodes = h->nbb;
+        a.axis = a.side = a.type = 0;
+        a.press = 0.0;
+        a.vel[0] = a.vel[1] = a.vel[2] = 0.0;
         a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
         a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
         a.lattice = h->p.lattice; a.highorder = h->p.highorder; a.tc = h->tc; a.dr = h->dr;
@@ -849,6 +871,7 @@ int handle_post_step(lbf_handle* h) {
         a.phi = h->tc ? h->phi[in] : nullptr;
         a.mom = h->mom[h->cur]; a.pres = h->pres[h->cur];
         for (int f = 0; f < lbf::NSCALE_H; ++f) a.scale[f] = h->scale[f];
+        if (h->nbb) CUDA_TRY(lbf::launch_bounce_back(h->storage, a, h->stream));
         for (int axis = 0; axis < 3; ++axis) {
             if (!(h->obc_open & (1 << axis))) continue;
             for (int side = 0; side < 2; ++side) {

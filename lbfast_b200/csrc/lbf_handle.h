@@ -47,6 +47,8 @@ struct lbf_handle {
     int tile_y = 8;      // rows of the kernel tile
     double* d_mass = nullptr;  // phi correction: {sum, count, sum at the first step, face flux} (FP64)
     int obc_open = 0;  // open faces (openbc, non-periodic axes): bit 0 x, 1 y, 2 z
+    long long* bb_nodes = nullptr;  // BOUNCE_BACK: the isfluid = -1 nodes
+    long long nbb = 0;
     bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
 };
 

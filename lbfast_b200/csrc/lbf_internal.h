@@ -119,19 +119,25 @@ cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const vo
 cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
                         cudaStream_t st);
 
-// Open face (axis 0/1/2, side 0 low / 1 high) after a step: replaces the
-// bounce-back populations of the wall links at the face's isfluid = -1 nodes
-// by those of the face's state, on the step's output moments
-// (boundary_cds_module.f90:57-1311).  The face nodes' moments after the force
-// half-step are recomputed from the step's input buffers, which the step
-// leaves intact.  One launch per face, in the reference's order x low,
-// x high, y low, ..., z high.
-struct OpenFaceArgs {
+// Wall passes after a step, on the step's output moments, at isfluid = -1
+// nodes; each recomputes its nodes' moments after the force half-step from the
+// step's input buffers, which the step leaves intact (lbf_walls.cu).
+//  * open face (axis 0/1/2, side 0 low / 1 high): replaces the bounce-back
+//    populations of the wall links by those of the face's state
+//    (boundary_cds_module.f90:57-1311); one launch per face, in the
+//    reference's order x low, x high, y low, ..., z high.
+//  * BOUNCE_BACK (lb_cuda_fused_module.f90:20-424): replaces the step's
+//    moment-space bounce-back of the wall links by the half-way bounce-back
+//    of the node's own post-collision populations, over the nodes of `nodes`.
+struct BoundaryArgs {
     int nx, ny, nz, pbx, pby, pbz;
     int axis, side, type;       // type: 2 zero gradient, 1 pressure, other velocity
     double press, vel[3];
     int lattice, highorder, tc, dr;
     double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
+    int smag;                   // SMAGORINSKI relaxation in the collision
+    const long long* nodes;     // BOUNCE_BACK: the isfluid = -1 nodes
+    long long nnodes;
     const int8_t* isf;
     const void* min;            // the step's input moments
     const float* pres_in;       // the step's input P (16-bit storage)
@@ -141,7 +147,8 @@ struct OpenFaceArgs {
     float* pres;                // the step's output P (16-bit storage)
     double scale[NSCALE_H];
 };
-cudaError_t launch_open_face(int storage, const OpenFaceArgs& a, cudaStream_t st);
+cudaError_t launch_open_face(int storage, const BoundaryArgs& a, cudaStream_t st);
+cudaError_t launch_bounce_back(int storage, const BoundaryArgs& a, cudaStream_t st);
 
 // phi carried through the open faces by a state (BCPHIFLUX,
 // boundary_cds_module.f90:1667-1861): sum over the isfluid = -1 nodes of the

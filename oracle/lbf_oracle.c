@@ -26,6 +26,7 @@
  *   fused collide+stream  lb_cuda_fused_module.f90:426-750
  *   update_phi            lb_cuda_update_phi_module.f90:19-104
  *   obstacle bounce-back  lb_cuda_boundary_module.f90:19-216
+ *   BOUNCE_BACK           lb_cuda_fused_module.f90:20-424 (half-way, in the streaming)
  *   open boundaries       boundary_cds_module.f90:57-1311 (moments), 1351-1663 (phi), 1667-1885 (flux)
  *   copy_print            print_module.f90:638-776
  *   lattice tables        vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15)
@@ -86,6 +87,7 @@ typedef struct orc_params {
     int obc_type[3][2];
     double obc_press[3][2];
     double obc_vel[3][2][3];
+    int bounce_back; /* BOUNCE_BACK: half-way bounce-back in the fused kernel (see fused) */
 } orc_params;
 
 /* ---- lattice tables: vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15) ---- */
@@ -720,12 +722,18 @@ static void collide_node(const orc_state *s, real **hin, const real *ph, long c,
 }
 
 /* fused_LB_kernel: every interior node x receives f*_l(x - c_l), summed in
- * link order into the ten output moments (lb_cuda_fused_module.f90:637-748). */
+ * link order into the ten output moments (lb_cuda_fused_module.f90:637-748).
+ * BOUNCE_BACK (fused_LB_kernel_bb, lb_cuda_fused_module.f90:364-380): a link
+ * whose upstream node x - c_l is solid (isfluid = 0) brings instead the
+ * node's own post-collision population of the opposite link -- the solid
+ * node sends back what it received from x, in the same step (half-way
+ * bounce-back); solid nodes push nothing (zeroed moments). */
 static void fused(orc_state *s, real **hin, real **hout, const real *ph)
 {
     const real cssq = (real)(1.0 / 3.0);
     const int NXY = s->NX * s->NY;
     const int nl = s->nl;
+    const int bb = s->p.obstacles && s->p.bounce_back;
     real *fst = (real *)malloc(sizeof(real) * (size_t)s->npad * (size_t)nl);
     int k;
     /* post-collision populations on the interior and its halo ring */
@@ -753,6 +761,7 @@ static void fused(orc_state *s, real **hin, real **hout, const real *ph)
                 for (l = 1; l < nl; l++) {
                     long src = c - s->ex[l] - (long)s->ey[l] * s->NX - (long)s->ez[l] * NXY;
                     real f = fst[(size_t)src * nl + l];
+                    if (bb && s->isf[src] == 0) f = fst[(size_t)c * nl + s->opp[l]];
                     real dex = (real)s->ex[l], dey = (real)s->ey[l], dez = (real)s->ez[l];
                     op = op + f;
                     ou = ou + f * dex; ov = ov + f * dey; ow = ow + f * dez;
@@ -1152,7 +1161,9 @@ static void one_step(orc_state *s)
     fused(s, A, B, pA);
     if (s->p.twocomp) update_phi(s, A, pA, pB);
     if (s->p.obstacles) {
-        obstacle_bb(s, A, B, pA);
+        /* bcs_mesoscopic_hfields: LB_int_boundary only without BOUNCE_BACK
+         * (boundary_cds_module.f90:50-56), then the open faces */
+        if (!s->p.bounce_back) obstacle_bb(s, A, B, pA);
         if (s->p.openbc) open_bc(s, A, B, pA);
     }
     if (s->p.twocomp) {

@@ -33,7 +33,7 @@ class OrcParams(C.Structure):
         ("tau_diff", C.c_double), ("fx", C.c_double), ("fy", C.c_double),
         ("fz", C.c_double), ("wettab_r", C.c_double), ("phi_correction", C.c_int), ("smagorinsky", C.c_int),
         ("openbc", C.c_int), ("obc_type", (C.c_int * 2) * 3), ("obc_press", (C.c_double * 2) * 3),
-        ("obc_vel", ((C.c_double * 3) * 2) * 3),
+        ("obc_vel", ((C.c_double * 3) * 2) * 3), ("bounce_back", C.c_int),
     ]
 
 
@@ -121,6 +121,7 @@ class Oracle:
         ty = params.get("openbc_type") or ((0, 0),) * 3
         pr = params.get("openbc_press") or ((0.0, 0.0),) * 3
         ve = params.get("openbc_vel") or (((0.0,) * 3,) * 2,) * 3
+        p.bounce_back = int(params.get("bounce_back", 0))
         for a in range(3):
             for sd in range(2):
                 p.obc_type[a][sd] = int(ty[a][sd])

@@ -56,10 +56,10 @@ def _spheres_solid(rng, shape, n, rmin, rmax):
 
 
 def make_case(name: str, storage: str = "f32"):
-    for suffix, flag in (("_corr", "phi_correction"), ("_smag", "smagorinsky")):
+    for suffix, flag in (("_corr", "phi_correction"), ("_smag", "smagorinsky"), ("_bb", "bounce_back")):
         if name.endswith(suffix):
             # the same case with the phi mass correction after every step / the
-            # Smagorinsky relaxation time
+            # Smagorinsky relaxation time / the half-way bounce-back
             p, isf, m, phi = make_case(name[: -len(suffix)], storage)
             setattr(p, flag, 1)
             return p, isf, m, phi
@@ -182,7 +182,8 @@ def make_case(name: str, storage: str = "f32"):
 ALL_CASES = ["tg_q19", "q27ho_1c_force", "q27_1c", "q27ho_2c_dr", "q27_2c_dr", "q19_2c_dr", "q27ho_2c", "q19_2c",
              "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr", "q27ho_1c_force_smag",
              "obs_q27ho_2c_dr_smag", "q19_2c_smag", "q15_1c", "q15_2c_dr", "obs_q15_2c_dr", "open_q27ho_2c_dr",
-             "open_q27_2c", "open_q15_2c_dr", "open_q19_1c", "open_q27ho_2c_dr_corr"]
+             "open_q27_2c", "open_q15_2c_dr", "open_q19_1c", "open_q27ho_2c_dr_corr", "obs_q27ho_2c_dr_bb",
+             "obs_q19_1c_bb", "obs_q15_2c_dr_bb", "obs_q27ho_2c_dr_smag_bb", "open_q19_1c_bb"]
 
 
 def run_oracle(name: str, nsteps: int, prec: str = "f64"):

@@ -255,6 +255,27 @@ def test_poiseuille_profile(lattice):
     assert err < 0.005, err
 
 
+@pytest.mark.parametrize("lattice", [19, 27])
+def test_poiseuille_profile_bounce_back(lattice):
+    """The POISEUILLE case with BOUNCE_BACK: the half-way bounce-back puts the
+    no-slip plane between the solid and the first fluid node, and the profile
+    matches the reference's parabola for it, H = (lx - 2)/2
+    (init_conditions_module.f90:248-252), within 0.5 % of its peak."""
+    lx, ly, lz, fz, nu = 64, 8, 32, 0.5e-5, 0.1
+    isf = L.mark_isfluid(np.ones((lz, ly, lx), np.int8), (0, 1, 1), lattice, True)
+    p = L.Params(lx=lx, ly=ly, lz=lz, pbc_x=0, lattice=lattice, obstacles=1, visc1=nu, fz=fz, bounce_back=1)
+    s = L.Solver(p)
+    s.set_isfluid(isf)
+    s.set_fields(np.zeros((10, lz, ly, lx)))
+    s.step(40000)
+    _, vel, _ = s.get_print()
+    s.close()
+    num = ST.poiseuille_profile(vel[2], isf)
+    th = ST.poiseuille_theory(lx, fz, nu, H=(lx - 2) / 2, xc=(lx + 1) / 2)
+    err = np.abs(num[1:-1] - th[1:-1]).max() / th.max()
+    assert err < 0.005, err
+
+
 def test_lamb_oscillation_frequency():
     """Lamb's n = 2 oscillation (the observable and theory of statistics.f90:
     377-471, 959-1050; sigma 0.03, nu 0.001, equal densities of lamb.inp) of

@@ -152,7 +152,7 @@ def test_raw_xdmf_writer(tmp_path):
 
 @pytest.mark.parametrize("bad", [dict(lattice=13), dict(highorder=1, lattice=19), dict(densratio=1),
                                  dict(lx=0), dict(storage="f8"), dict(visc1=-1.0), dict(openbc=1, pbc_x=0),
-                                 dict(openbc=1, obstacles=1, pbc_y=0, ly=2)])
+                                 dict(openbc=1, obstacles=1, pbc_y=0, ly=2), dict(bounce_back=1)])
 def test_create_rejects_invalid_parameters_before_device_work(bad):
     kw = dict(lx=8, ly=8, lz=8, lattice=27)
     kw.update(bad)

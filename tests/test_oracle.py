@@ -200,3 +200,24 @@ def test_open_velocity_inlet_conserves_the_flow_rate():
     inner = q[10:lx - 10]  # planes away from the faces' distortion
     assert inner.min() > 0
     assert (inner.max() - inner.min()) < 1e-3 * inner.mean()
+
+
+@pytest.mark.parametrize("bb,H_off", [(0, 1), (1, 2)])
+def test_poiseuille_wall_position(bb, H_off):
+    """Body-force Poiseuille between walls at y = 0 and ly-1: the moment-space
+    bounce-back (LB_int_boundary) puts the no-slip plane on the solid rows,
+    H = (ly-1)/2; BOUNCE_BACK half way between solid and fluid, H = (ly-2)/2
+    (init_conditions_module.f90:248-252)."""
+    lx, ly, lz, nu, fx = 4, 18, 4, 0.1, 1e-6
+    isf = O.mark_isfluid(np.zeros((lz, ly, lx), bool), (1, 0, 1), 19, True)
+    o = O.Oracle(dict(lx=lx, ly=ly, lz=lz, pbc_x=1, pbc_y=0, pbc_z=1, lattice=19, obstacles=1, visc1=nu, fx=fx,
+                      bounce_back=bb))
+    o.set_isfluid(isf)
+    o.set_fields(np.zeros((10, lz, ly, lx)))
+    o.step(6000)
+    h, _, _ = o.get_fields()
+    y = np.arange(ly)
+    H, yc = (ly - H_off) / 2, (ly - 1) / 2
+    theory = fx / (2 * nu) * (H * H - (y - yc) ** 2)
+    u = h[1, 1, :, 1]
+    assert np.abs(u[1:-1] - theory[1:-1]).max() < 0.01 * theory.max()
