@@ -100,6 +100,12 @@ typedef struct lbf_params {
                                 node is solid brings the node's own post-collision population of the opposite
                                 link (fused_LB_kernel_bb, lb_cuda_fused_module.f90:20-424) -- instead of the
                                 moment-space correction of LB_int_boundary */
+    int repulsive_flux;      /* REPULSIVE_FLUX (requires twocomponent): before each step every interfacial node
+                                pairs with the nearest facing interface within 3 nodes and gets a film
+                                repulsion force, added (capped at 1e-3) in the moments prologue
+                                (lb_cuda_repulsive_module.f90:19-292, lb_cuda_moments_module.f90:148-160) */
+    double a_rep, cos_opp_t, q_th;  /* A_rep, cosOppT, q_th of the &fluid namelist: strength, facing threshold
+                                       of n1 . n2, interface threshold of phi (1 - phi) */
 } lbf_params;
 
 typedef struct lbf_handle lbf_handle;

@@ -44,7 +44,8 @@ class LbfParams(C.Structure):
         ("printphi", C.c_int), ("zseg", C.c_int), ("tile_y", C.c_int), ("phi_correction", C.c_int),
         ("smagorinsky", C.c_int), ("openbc", C.c_int), ("openbc_type", (C.c_int * 2) * 3),
         ("openbc_press", (C.c_double * 2) * 3), ("openbc_vel", ((C.c_double * 3) * 2) * 3),
-        ("bounce_back", C.c_int),
+        ("bounce_back", C.c_int), ("repulsive_flux", C.c_int), ("a_rep", C.c_double), ("cos_opp_t", C.c_double),
+        ("q_th", C.c_double),
     ]
 
 
@@ -173,6 +174,10 @@ class Params:
     openbc_press: tuple = ((0.0, 0.0), (0.0, 0.0), (0.0, 0.0))
     openbc_vel: tuple = (((0.0,) * 3,) * 2,) * 3
     bounce_back: int = 0  # half-way bounce-back at obstacles (BOUNCE_BACK)
+    repulsive_flux: int = 0  # film repulsion between facing interfaces (REPULSIVE_FLUX)
+    a_rep: float = 0.0
+    cos_opp_t: float = 0.0
+    q_th: float = 0.0
 
     def to_c(self) -> LbfParams:
         p = LbfParams()

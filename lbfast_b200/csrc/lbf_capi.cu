@@ -90,6 +90,8 @@ void free_all(lbf_handle* h) {
     cudaFree(h->d_red);
     cudaFree(h->d_mass);
     cudaFree(h->bb_nodes);
+    cudaFree(h->d_rnrm);
+    cudaFree(h->d_rep);
     cudaFree(h->staging);
 }
 
@@ -140,7 +142,7 @@ int autotune(lbf_handle* h) {
         if (it != g_tune_cache.end()) {
             h->tile_y = it->second.first;
             h->zseg = it->second.second;
-            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, h->tile_y);
+            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->tile_y);
             return LBF_OK;
         }
     }
@@ -168,7 +170,7 @@ int autotune(lbf_handle* h) {
     std::pair<int, int> pick(h->tile_y, h->zseg);
     int rc = LBF_OK;
     for (const auto& c : cand) {
-        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, c.first);
+        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), c.first);
         if (!L) continue;
         lbf::StepArgs a;
         const int zs0 = h->zseg;
@@ -196,7 +198,7 @@ int autotune(lbf_handle* h) {
     if (rc) return rc;
     h->tile_y = pick.first;
     h->zseg = pick.second;
-    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, h->p.twocomponent, h->tile_y);
+    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->tile_y);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = pick;
     return LBF_OK;
@@ -321,6 +323,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     // bcs_mesoscopic_hfields / _phifields run only with INTERNAL_OBSTACLES (integrator_module.f90:514-523)
     if (p->openbc && !p->obstacles) return fail(LBF_E_ARG, "openbc requires obstacles (INTERNAL_OBSTACLES)");
     if (p->bounce_back && !p->obstacles) return fail(LBF_E_ARG, "bounce_back requires obstacles (INTERNAL_OBSTACLES)");
+    if (p->repulsive_flux && !p->twocomponent) return fail(LBF_E_ARG, "repulsive_flux requires TWOCOMPONENT");
     // an open axis holds a wall, the face plane and a wall at least
     if (p->openbc && ((!p->pbc_x && p->lx < 3) || (!p->pbc_y && p->ly < 3) || (!p->pbc_z && p->lz < 3)))
         return fail(LBF_E_ARG, "openbc: a non-periodic axis needs at least 3 nodes");
@@ -362,7 +365,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     // 16 rows do not fit in shared memory); tile_y = 0 also tunes the schedule
     h->tile_y = p->tile_y ? p->tile_y : (lbf::tile_available(p->storage, 16) ? 16 : 8);
     h->tuned = p->tile_y != 0;
-    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, p->twocomponent, h->tile_y);
+    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, lbf::kernel_tc(*p), h->tile_y);
     if (!h->launcher) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
@@ -380,6 +383,10 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (ok) ok = cudaMalloc(&h->d_red, 5 * sizeof(double)) == cudaSuccess;
     if (ok && p->phi_correction) ok = cudaMalloc(&h->d_mass, 4 * sizeof(double)) == cudaSuccess;
     if (p->openbc) h->obc_open = (p->pbc_x ? 0 : 1) | (p->pbc_y ? 0 : 2) | (p->pbc_z ? 0 : 4);
+    if (ok && p->repulsive_flux) {
+        ok = cudaMalloc(&h->d_rnrm, 3 * h->N * sizeof(double)) == cudaSuccess;
+        if (ok) ok = cudaMalloc(&h->d_rep, 3 * h->N * (p->storage == LBF_STORE_F64 ? 8 : 4)) == cudaSuccess;
+    }
     if (!ok) {
         cudaGetLastError();
         free_all(h);
@@ -650,7 +657,7 @@ int lbf_step(lbf_handle* h, int nsteps) {
     }
     lbf::StepArgs a;
     for (int s = 0; s < nsteps; ++s) {
-        int rc = launch_wet(h, h->cur, 1 - h->cur, false);
+        int rc = lbf::handle_pre_step(h);
         if (rc) return rc;
         const bool write_u = h->dr || s == nsteps - 1;
         lbf::handle_step_args(h, a, write_u);
@@ -815,6 +822,7 @@ void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u) {
     for (int i = 0; i < NSCALE_H; ++i) a.scale[i] = h->scale[i];
     a.isf = h->obs ? h->isf : nullptr;
     a.err = h->d_err;
+    a.rep = h->d_rep;
     a.min = h->mom[in];
     a.mout = h->mom[out];
     a.uin = h->uold[in];
@@ -841,10 +849,25 @@ size_t handle_bytes(const lbf_params* p) {
     if (half) b += 2 * N * sizeof(float);
     if (p->obstacles) b += N;
     if (p->phi_correction) b += 4 * sizeof(double);
+    if (p->repulsive_flux) b += 3 * N * (sizeof(double) + (p->storage == LBF_STORE_F64 ? 8 : 4));
     return b;
 }
 
-int handle_pre_step(lbf_handle* h) { return launch_wet(h, h->cur, 1 - h->cur, false); }
+int handle_pre_step(lbf_handle* h) {
+    int rc = launch_wet(h, h->cur, 1 - h->cur, false);
+    if (rc || !h->d_rep) return rc;
+    // REPULSIVE_FLUX force of this step from its input phi (integrator_module.f90:325-328)
+    lbf::RepulsiveArgs a;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
+    a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
+    a.width = h->p.width; a.a_rep = h->p.a_rep; a.cos_opp_t = h->p.cos_opp_t; a.q_th = h->p.q_th;
+    a.isf = h->obs ? h->isf : nullptr;
+    a.phi = h->phi[h->cur];
+    a.nrm = h->d_rnrm;
+    a.force = h->d_rep;
+    CUDA_TRY(lbf::launch_repulsive(h->storage, a, h->stream));
+    return LBF_OK;
+}
 
 int handle_post_step(lbf_handle* h) {
     // wall passes on the step's output moments (buffer cur after the advance),
@@ -854,6 +877,7 @@ int handle_post_step(lbf_handle* h) {
         const int in = 1 - h->cur;
         lbf::BoundaryArgs a;
         a.smag = h->p.smagorinsky;
+        a.rep = h->d_rep;
         a.nodes = h->bb_nodes;
         a.nnodes = h->nbb;
         a.axis = a.side = a.type = 0;

@@ -49,6 +49,8 @@ struct lbf_handle {
     int obc_open = 0;  // open faces (openbc, non-periodic axes): bit 0 x, 1 y, 2 z
     long long* bb_nodes = nullptr;  // BOUNCE_BACK: the isfluid = -1 nodes
     long long nbb = 0;
+    double* d_rnrm = nullptr;  // REPULSIVE_FLUX: normals (3 x N, FP64)
+    void* d_rep = nullptr;     // REPULSIVE_FLUX: force of the step (3 x N, arithmetic type)
     bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
 };
 

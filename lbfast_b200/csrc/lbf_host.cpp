@@ -378,6 +378,7 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
     p->tau_diff = 0.0;
     p->wettab_r = 90.0;
     p->openbc = 0;  // vars_module.f90:238-255
+    p->a_rep = p->cos_opp_t = p->q_th = 0.0;
     for (int a = 0; a < 3; ++a)
         for (int sd = 0; sd < 2; ++sd) {
             p->openbc_type[a][sd] = 0;
@@ -456,8 +457,11 @@ extern "C" int lbf_read_namelists(const char* path, lbf_params* p, lbf_run* run)
             else if (k == "rho_r") p->rho_r = to_real(a, k);
             else if (k == "rho_b") p->rho_b = to_real(a, k);
             else if (k == "uwall") run->uwall = to_real(a, k);
+            else if (k == "a_rep") p->a_rep = to_real(a, k);  // REPULSIVE_FLUX (LBFAST.f90:57-58)
+            else if (k == "cosoppt") p->cos_opp_t = to_real(a, k);
+            else if (k == "q_th") p->q_th = to_real(a, k);
             else if (k == "wettab_b" || k == "mu_max" || k == "ks" || k == "k_elastic" || k == "lambda_rel" ||
-                     k == "rhoin" || k == "rhoout" || k == "a_rep" || k == "cosoppt" || k == "q_th") {
+                     k == "rhoin" || k == "rhoout") {
                 for (auto& x : v) to_real(x, k);
             } else if (k == "npoint" || k == "ndir") { for (auto& x : v) to_int(x, k); }
             else throw NmlError{"unknown key `" + k + "` in &fluid"};

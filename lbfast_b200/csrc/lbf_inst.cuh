@@ -37,14 +37,15 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.pres_out = a.pres_out;
     p.isf = a.isf;
     p.err = a.err;
+    p.rep = static_cast<const R*>(a.rep);
 }
 
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
 cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     static bool attr_set = false;
     const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV, REP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
@@ -53,48 +54,48 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     make_params(a, p);
     if (a.zseg > 0) {
         dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
-        stream_kernel<LAT, HO, TC, S, R, TYV><<<grid, TX * TYV, smem, st>>>(p);
+        stream_kernel<LAT, HO, TC, S, R, TYV, REP><<<grid, TX * TYV, smem, st>>>(p);
         return cudaGetLastError();
     }
     static int resident = 0;  // CTAs per SM at this shared-memory size
     if (!resident) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel<LAT, HO, TC, S, R, TYV>,
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel<LAT, HO, TC, S, R, TYV, REP>,
                                                                       TX * TYV, smem);
         if (e != cudaSuccess) return e;
         if (resident < 1) return cudaErrorInvalidConfiguration;
     }
     const long long W = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV) * a.nz;
     const int grid = persistent_grid(W, resident);
-    stream_kernel<LAT, HO, TC, S, R, TYV><<<grid, TX * TYV, smem, st>>>(p);
+    stream_kernel<LAT, HO, TC, S, R, TYV, REP><<<grid, TX * TYV, smem, st>>>(p);
     return cudaGetLastError();
 }
 
 // One launch advancing many boxes of one kernel class: d_boxes holds one
 // StepParams per box, d_work one (box, first column-plane, end column-plane)
 // per CTA.
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
 cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st) {
     static bool attr_set = false;
     const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (nwork <= 0) return cudaSuccess;
-    stream_kernel_batched<LAT, HO, TC, S, R, TYV>
+    stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>
         <<<nwork, TX * TYV, smem, st>>>(static_cast<const StepParams<S, R>*>(d_boxes), d_work);
     return cudaGetLastError();
 }
 
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV> int batched_resident() {
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false> int batched_resident() {
     static int resident = 0;
     if (!resident) {
         const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
-        if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
+        if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV>,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
                                                           TX * TYV, smem) != cudaSuccess)
             resident = 1;
         resident = std::max(resident, 1);
@@ -106,15 +107,32 @@ template <typename S, typename R> void fill_params(const StepArgs& a, void* dst)
     make_params(a, *static_cast<StepParams<S, R>*>(dst));
 }
 
-// the five kernel classes of one storage type and tile height
+// the kernel classes of one storage type and tile height; tc: 0 one
+// component, 1 two components, 2 two components with REPULSIVE_FLUX
+template <int LAT, bool HO, typename S, typename R, int TYV> StepLauncher step_class(int tc) {
+    return tc == 2 ? &launch_stream<LAT, HO, true, S, R, TYV, true>
+                   : tc ? &launch_stream<LAT, HO, true, S, R, TYV> : &launch_stream<LAT, HO, false, S, R, TYV>;
+}
 template <typename S, typename R, int TYV> StepLauncher step_table(int lat, int ho, int tc) {
-    if (lat == 15 && !ho) return tc ? &launch_stream<15, false, true, S, R, TYV> : &launch_stream<15, false, false, S, R, TYV>;
-    if (lat == 19 && !ho) return tc ? &launch_stream<19, false, true, S, R, TYV> : &launch_stream<19, false, false, S, R, TYV>;
-    if (lat == 27 && ho) return tc ? &launch_stream<27, true, true, S, R, TYV> : &launch_stream<27, true, false, S, R, TYV>;
-    if (lat == 27 && !ho) return tc ? &launch_stream<27, false, true, S, R, TYV> : &launch_stream<27, false, false, S, R, TYV>;
+    if (lat == 15 && !ho) return step_class<15, false, S, R, TYV>(tc);
+    if (lat == 19 && !ho) return step_class<19, false, S, R, TYV>(tc);
+    if (lat == 27 && ho) return step_class<27, true, S, R, TYV>(tc);
+    if (lat == 27 && !ho) return step_class<27, false, S, R, TYV>(tc);
     return nullptr;
 }
 
+template <int LAT, bool HO, typename S, typename R, int TYV> void batch_class(int tc, BatchOps& o) {
+    if (tc == 2) {
+        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV, true>;
+        o.resident = &batched_resident<LAT, HO, true, S, R, TYV, true>;
+    } else if (tc) {
+        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV>;
+        o.resident = &batched_resident<LAT, HO, true, S, R, TYV>;
+    } else {
+        o.launch = &launch_stream_batched<LAT, HO, false, S, R, TYV>;
+        o.resident = &batched_resident<LAT, HO, false, S, R, TYV>;
+    }
+}
 template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho, int tc) {
     BatchOps o;
     o.params_bytes = sizeof(StepParams<S, R>);
@@ -122,22 +140,10 @@ template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho,
     o.tile_y = TYV;
     o.launch = nullptr;
     o.resident = nullptr;
-    if (lat == 15 && !ho) {
-        o.launch = tc ? &launch_stream_batched<15, false, true, S, R, TYV> : &launch_stream_batched<15, false, false, S, R, TYV>;
-        o.resident = tc ? &batched_resident<15, false, true, S, R, TYV> : &batched_resident<15, false, false, S, R, TYV>;
-    }
-    if (lat == 19 && !ho) {
-        o.launch = tc ? &launch_stream_batched<19, false, true, S, R, TYV> : &launch_stream_batched<19, false, false, S, R, TYV>;
-        o.resident = tc ? &batched_resident<19, false, true, S, R, TYV> : &batched_resident<19, false, false, S, R, TYV>;
-    }
-    if (lat == 27 && ho) {
-        o.launch = tc ? &launch_stream_batched<27, true, true, S, R, TYV> : &launch_stream_batched<27, true, false, S, R, TYV>;
-        o.resident = tc ? &batched_resident<27, true, true, S, R, TYV> : &batched_resident<27, true, false, S, R, TYV>;
-    }
-    if (lat == 27 && !ho) {
-        o.launch = tc ? &launch_stream_batched<27, false, true, S, R, TYV> : &launch_stream_batched<27, false, false, S, R, TYV>;
-        o.resident = tc ? &batched_resident<27, false, true, S, R, TYV> : &batched_resident<27, false, false, S, R, TYV>;
-    }
+    if (lat == 15 && !ho) batch_class<15, false, S, R, TYV>(tc, o);
+    if (lat == 19 && !ho) batch_class<19, false, S, R, TYV>(tc, o);
+    if (lat == 27 && ho) batch_class<27, true, S, R, TYV>(tc, o);
+    if (lat == 27 && !ho) batch_class<27, false, S, R, TYV>(tc, o);
     return o;
 }
 

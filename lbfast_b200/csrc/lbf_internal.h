@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "../../include/lbfast_gpu.h"
+
 namespace lbf {
 
 constexpr int NSCALE_H = 14;
@@ -24,6 +26,7 @@ struct StepArgs {
     float* pres_out;
     const int8_t* isf;
     int* err;
+    const void* rep;        // REPULSIVE_FLUX force of the step (3 x N, arithmetic type), or nullptr
 };
 
 using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
@@ -31,6 +34,9 @@ using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
 // Step launcher of one kernel class (lattice 19/27, HIGHORDER, TWOCOMPONENT)
 // for a storage type and tile height (8 or 16 rows); nullptr if not built.
 StepLauncher step_launcher(int storage, int lat, int ho, int tc, int tile_y);
+// kernel class argument `tc` of a run: 0 one component, 1 two components,
+// 2 two components with REPULSIVE_FLUX (its own compilation of the step)
+inline int kernel_tc(const lbf_params& p) { return p.twocomponent ? (p.repulsive_flux ? 2 : 1) : 0; }
 bool tile_available(int storage, int tile_y);
 
 // Batched step of many boxes of one kernel class and tile height: fill writes
@@ -136,6 +142,7 @@ struct BoundaryArgs {
     int lattice, highorder, tc, dr;
     double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     int smag;                   // SMAGORINSKI relaxation in the collision
+    const void* rep;            // REPULSIVE_FLUX force of the step (3 x N, arithmetic type), or nullptr
     const long long* nodes;     // BOUNCE_BACK: the isfluid = -1 nodes
     long long nnodes;
     const int8_t* isf;
@@ -155,6 +162,18 @@ cudaError_t launch_bounce_back(int storage, const BoundaryArgs& a, cudaStream_t 
 // planes next to the walls of +-u_n phi, into d_flux (set, not added)
 cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const void* phi,
                             const int8_t* isf, const double* inv_scale, double* d_flux, cudaStream_t st);
+
+// REPULSIVE_FLUX before a step (lbf_repulsive.cu): the film-repulsion force
+// of every node from the step's input phi into `force`
+struct RepulsiveArgs {
+    int nx, ny, nz, pbx, pby, pbz;
+    double width, a_rep, cos_opp_t, q_th;
+    const int8_t* isf;          // nullptr without obstacles
+    const void* phi;            // the step's input phi
+    double* nrm;                // 3 x N normals (work array)
+    void* force;                // 3 x N force, arithmetic type of the storage
+};
+cudaError_t launch_repulsive(int storage, const RepulsiveArgs& a, cudaStream_t st);
 
 size_t storage_bytes(int storage);
 

@@ -141,6 +141,7 @@ template <typename S, typename R> struct StepParams {
     typename PhiStore<S>::type* pout;       // N phase field, output (fluid nodes)
     const int8_t* isf;  // N isfluid (obstacles), else nullptr
     int* err;         // device error word
+    const R* rep;     // REPULSIVE_FLUX force (3 x N), else nullptr
 };
 
 }  // namespace lbf

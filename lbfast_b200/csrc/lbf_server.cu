@@ -194,7 +194,7 @@ int rebuild(lbf_server* s) {
     drop_graph(s);
     for (auto& kv : s->batches) kv.second.members.clear();
     for (Solve* v : s->active) {
-        ClassKey k{v->p.lattice, v->p.highorder, v->p.twocomponent, v->p.storage, solve_tile(v->p)};
+        ClassKey k{v->p.lattice, v->p.highorder, lbf::kernel_tc(v->p), v->p.storage, solve_tile(v->p)};
         Batch& b = s->batches[k];
         if (!b.ops.launch) {
             b.ops = lbf::batch_ops(k.storage, k.lat, k.ho, k.tc, k.tile);

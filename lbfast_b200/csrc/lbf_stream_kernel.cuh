@@ -79,7 +79,9 @@ template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t st
 }
 
 // One piece of a time step: tile (bx, by) of the box, planes z0 <= z < z1.
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+// REP: REPULSIVE_FLUX force in the moments prologue (a separate compilation,
+// so the kernels without it carry no code for it).
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
 __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int bx, const int by, const int z0,
                                           const int z1) {
     using TL = Tile<TYV>;
@@ -486,6 +488,19 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     fxv += chem * gfx;
                     fyv += chem * gfy;
                     fzv += chem * gfz;
+                    if constexpr (REP) {
+                        // REPULSIVE_FLUX (lb_cuda_moments_module.f90:148-160): rho_phi F_rep,
+                        // each component capped at 1e-3, times rho_phi
+                        const R rh = dr ? p.rho_r * phi + (R(1) - phi) * p.rho_b : R(1);
+                        const R cap = R(1.0e-3);
+                        R t0 = p.rep[gi] * rh, t1 = p.rep[N + gi] * rh, t2 = p.rep[2 * N + gi] * rh;
+                        t0 = t0 > cap ? cap : (t0 < -cap ? -cap : t0);
+                        t1 = t1 > cap ? cap : (t1 < -cap ? -cap : t1);
+                        t2 = t2 > cap ? cap : (t2 < -cap ? -cap : t2);
+                        fxv += t0 * rh;
+                        fyv += t1 * rh;
+                        fzv += t2 * rh;
+                    }
                 }
                 if (dr) {
                     const R drho = p.rho_r - p.rho_b;
@@ -795,7 +810,7 @@ __device__ __forceinline__ void run_share(const int nx, const int ny, const int 
 // site of step_body, so the kernel holds a single compiled copy of the step:
 // separately inlined copies may contract floating-point operations
 // differently and give results that differ in the last bit.
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
     long long s0, s1;
     if (p.zseg > 0) {
@@ -810,14 +825,14 @@ __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_ke
         s1 = min(W, s0 + share);
     }
     run_share<TYV>(p.nx, p.ny, p.nz, s0, s1,
-                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV>(p, bx, by, z0, z1); });
+                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV, REP>(p, bx, by, z0, z1); });
 }
 
 // Many boxes in one launch: CTA i advances box work[i].x over column-planes
 // [work[i].y, work[i].z) of that box (column-major: plane fastest), with the
 // box's own parameters and fields.  Each node's arithmetic is the same as in
 // stream_kernel, so a box gives the same bits alone and in a batch.
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     stream_kernel_batched(const StepParams<S, R>* __restrict__ boxes, const int4* __restrict__ work) {
     __shared__ StepParams<S, R> sp;
@@ -825,7 +840,7 @@ __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     if (threadIdx.x == 0) sp = boxes[w.x];
     __syncthreads();
     run_share<TYV>(sp.nx, sp.ny, sp.nz, w.y, w.z,
-                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV>(sp, bx, by, z0, z1); });
+                   [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV, REP>(sp, bx, by, z0, z1); });
 }
 
 }  // namespace lbf

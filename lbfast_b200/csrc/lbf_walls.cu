@@ -189,6 +189,16 @@ __device__ void node_state(const BoundaryArgs& a, int x, int y, int z, long long
     if (a.tc) {
         const double chem = 4.0 * a.beta * phi * (phi - 1.0) * (phi - 0.5) - a.kapp * lap;
         fxv += chem * gfx; fyv += chem * gfy; fzv += chem * gfz;
+        if (a.rep) {  // REPULSIVE_FLUX (lb_cuda_moments_module.f90:148-160)
+            using R = typename std::conditional<sizeof(S) == 8, double, float>::type;
+            const R* rp = static_cast<const R*>(a.rep);
+            double t[3];
+            for (int d = 0; d < 3; ++d) {
+                t[d] = (double)rp[d * N + g] * rhophi;
+                if (fabs(t[d]) > 1.0e-3) t[d] = t[d] > 0 ? 1.0e-3 : -1.0e-3;
+            }
+            fxv += t[0] * rhophi; fyv += t[1] * rhophi; fzv += t[2] * rhophi;
+        }
     }
     if (a.dr) {
         grx = (a.rho_r - a.rho_b) * gfx; gry = (a.rho_r - a.rho_b) * gfy; grz = (a.rho_r - a.rho_b) * gfz;

@@ -27,6 +27,7 @@
  *   update_phi            lb_cuda_update_phi_module.f90:19-104
  *   obstacle bounce-back  lb_cuda_boundary_module.f90:19-216
  *   BOUNCE_BACK           lb_cuda_fused_module.f90:20-424 (half-way, in the streaming)
+ *   REPULSIVE_FLUX        lb_cuda_repulsive_module.f90:19-292; lb_cuda_moments_module.f90:148-160
  *   open boundaries       boundary_cds_module.f90:57-1311 (moments), 1351-1663 (phi), 1667-1885 (flux)
  *   copy_print            print_module.f90:638-776
  *   lattice tables        vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15)
@@ -88,6 +89,10 @@ typedef struct orc_params {
     double obc_press[3][2];
     double obc_vel[3][2][3];
     int bounce_back; /* BOUNCE_BACK: half-way bounce-back in the fused kernel (see fused) */
+    /* REPULSIVE_FLUX (see repulsive): switch and the A_rep, cosOppT, q_th of
+     * the input file (LBFAST.f90:57-58) */
+    int repulsive;
+    double a_rep, cos_opp_t, q_th;
 } orc_params;
 
 /* ---- lattice tables: vars_module.f90:319-338 (D3Q27), 666-684 (D3Q19), 685-703 (D3Q15) ---- */
@@ -112,6 +117,7 @@ typedef struct orc_state {
     real *aux[7];
     real *loc[2];
     real *frc[3];
+    real *rep[3];              /* REPULSIVE_FLUX force of the step (locauxfields 6-8) */
     int flip;                  /* index of the buffer that is the input of the next step */
     double phi_sum0;           /* sum of phi over fluid nodes at the first step */
     long step;
@@ -255,6 +261,7 @@ orc_state *orc_create(const orc_params *p)
     for (f = 0; f < 7; f++) s->aux[f] = zalloc(s->npad);
     for (f = 0; f < 2; f++) s->loc[f] = zalloc(s->npad);
     for (f = 0; f < 3; f++) s->frc[f] = zalloc(s->npad);
+    for (f = 0; f < 3; f++) s->rep[f] = zalloc(s->npad);
     s->prt_rho = zalloc(s->npad);
     s->prt_press = zalloc(s->npad);
     for (f = 0; f < 3; f++) s->prt_vel[f] = zalloc(s->npad);
@@ -274,6 +281,7 @@ void orc_destroy(orc_state *s)
     for (f = 0; f < 7; f++) free(s->aux[f]);
     for (f = 0; f < 2; f++) free(s->loc[f]);
     for (f = 0; f < 3; f++) free(s->frc[f]);
+    for (f = 0; f < 3; f++) free(s->rep[f]);
     free(s->prt_rho); free(s->prt_press);
     for (f = 0; f < 3; f++) free(s->prt_vel[f]);
     free(s);
@@ -529,6 +537,115 @@ static void wetting(orc_state *s, real *ph)
     }
 }
 
+/* index of node (i, j, k) folded into the box on periodic axes; -1 beyond a
+ * non-periodic face (the reference's halo layers there: isfluid 1, phi 0,
+ * aux 0) */
+static long wrap_index(const orc_state *s, int i, int j, int k)
+{
+    int c[3] = {i, j, k}, d;
+    const int n[3] = {s->nx, s->ny, s->nz}, pb[3] = {s->p.pbc_x, s->p.pbc_y, s->p.pbc_z};
+    for (d = 0; d < 3; d++)
+        if (c[d] < 0 || c[d] >= n[d]) {
+            if (!pb[d]) return -1;
+            c[d] = ((c[d] % n[d]) + n[d]) % n[d];
+        }
+    return IDX(s, c[0], c[1], c[2]);
+}
+
+/* REPULSIVE_FLUX: thinfilm_scan_mark_kernel and repulsive_flux_normal_kernel
+ * (lb_cuda_repulsive_module.f90:19-292), on the step's phi and the normals of
+ * compute_norm (aux 1-3).  An interfacial fluid node (q = phi (1 - phi) of
+ * the clamped phi >= q_th) looks in the window of +-3 nodes (LBFAST.f90:221)
+ * for the nearest fluid node of similar q (within 10 %) whose normal faces its
+ * own (n1 . n2 <= cosOppT), ties to the larger facing factor; the pair gives a
+ * force along the bisector of the two normals, of strength
+ * A_rep / (1 + W^4) qcl face with W = width arcosh(1 / (2 sqrt(qcl))) the
+ * film thickness, capped by phi / (1.5 |F|_1). */
+static void repulsive(orc_state *s, const real *ph)
+{
+    const double eps = 1.0e-9, q_th = s->p.q_th;
+    int k;
+#pragma omp parallel for schedule(static)
+    for (k = 0; k < s->nz; k++) {
+        int i, j, d;
+        for (j = 0; j < s->ny; j++)
+            for (i = 0; i < s->nx; i++) {
+                long c = IDX(s, i, j, k);
+                if (abs(s->isf[c]) != 1) continue;
+                for (d = 0; d < 3; d++) s->rep[d][c] = 0;
+                /* scan and mark (lb_cuda_repulsive_module.f90:63-150) */
+                double qloc = (double)ph[c];
+                qloc = qloc < 0 ? 0 : (qloc > 1 ? 1 : qloc);
+                qloc = qloc * (1.0 - qloc);
+                if (qloc < q_th) continue;
+                double nix = s->aux[0][c], niy = s->aux[1][c], niz = s->aux[2][c];
+                double best_r2 = 1.0e300, best_face = -1.0;
+                int bi = 0, bj = 0, bk = 0, found = 0, di, dj, dk;
+                for (di = -3; di <= 3; di++)
+                    for (dj = -3; dj <= 3; dj++)
+                        for (dk = -3; dk <= 3; dk++) {
+                            if (di == 0 && dj == 0 && dk == 0) continue;
+                            long nb = wrap_index(s, i + di, j + dj, k + dk);
+                            int fnb = nb < 0 ? 1 : s->isf[nb];
+                            if (abs(fnb) != 1) continue;
+                            double r2 = (double)di * di + (double)dj * dj + (double)dk * dk;
+                            if (r2 < 1.0e-12) continue;
+                            double qn = nb < 0 ? 0.0 : (double)ph[nb];
+                            qn = qn < 0 ? 0 : (qn > 1 ? 1 : qn);
+                            qn = qn * (1.0 - qn);
+                            if (qn < q_th || fabs(qn - qloc) > 0.1 * (qloc > 1.0e-12 ? qloc : 1.0e-12)) continue;
+                            double dotn = nb < 0 ? 0.0 : nix * s->aux[0][nb] + niy * s->aux[1][nb] + niz * s->aux[2][nb];
+                            if (dotn > s->p.cos_opp_t) continue;
+                            double face = 0.5 * (1.0 - dotn);
+                            if (r2 < best_r2 - 1.0e-14) {
+                                best_r2 = r2; best_face = face; bi = di; bj = dj; bk = dk; found = 1;
+                            } else if (fabs(r2 - best_r2) <= 1.0e-14 && face > best_face) {
+                                best_face = face; bi = di; bj = dj; bk = dk; found = 1;
+                            }
+                        }
+                if (!found) continue;
+                /* normal repulsive flux (lb_cuda_repulsive_module.f90:194-289) */
+                double loc_phi = (double)ph[c];
+                double q1 = loc_phi * (1.0 - loc_phi);
+                if (q1 <= eps) continue;
+                double dx = bi, dy = bj, dz = bk, r = sqrt(dx * dx + dy * dy + dz * dz);
+                if (r <= eps) continue;
+                dx /= r; dy /= r; dz /= r;
+                long nb = wrap_index(s, i + bi, j + bj, k + bk);
+                double n2x = nb < 0 ? 0 : s->aux[0][nb], n2y = nb < 0 ? 0 : s->aux[1][nb], n2z = nb < 0 ? 0 : s->aux[2][nb];
+                double face = -(nix * n2x + niy * n2y + niz * n2z);
+                if (face < 0) face = 0;
+                if (face <= eps) continue;
+                double nsx = nix - n2x, nsy = niy - n2y, nsz = niz - n2z;
+                double nsm = sqrt(nsx * nsx + nsy * nsy + nsz * nsz);
+                if (nsm <= eps) {
+                    nsx = dx; nsy = dy; nsz = dz;
+                } else {
+                    nsx /= nsm; nsy /= nsm; nsz /= nsm;
+                }
+                if (dx * nsx + dy * nsy + dz * nsz < 0) { nsx = -nsx; nsy = -nsy; nsz = -nsz; }
+                double phi2 = nb < 0 ? 0.0 : (double)ph[nb];
+                double q2 = phi2 * (1.0 - phi2), qpair = 0.5 * (q1 + q2);
+                double qcl = qpair > eps ? qpair : eps;
+                if (qcl > 0.25 - eps) qcl = 0.25 - eps;
+                double arg = 1.0 / (2.0 * sqrt(qcl));
+                if (arg <= 1.0) continue;
+                double wfilm = s->p.width * log(arg + sqrt(arg * arg - 1.0));
+                if (wfilm <= 0) continue;
+                double wd = 1.0 / (1.0 + pow(wfilm, 4.0));
+                double fx = s->p.a_rep * wd * qcl * face * nsx;
+                double fy = s->p.a_rep * wd * qcl * face * nsy;
+                double fz = s->p.a_rep * wd * qcl * face * nsz;
+                double cap = 1.5 * (fabs(fx) + fabs(fy) + fabs(fz));
+                double sc = loc_phi / (cap > 1.0e-9 ? cap : 1.0e-9);
+                if (sc > 1.0) sc = 1.0;
+                s->rep[0][c] = (real)(fx * sc);
+                s->rep[1][c] = (real)(fy * sc);
+                s->rep[2][c] = (real)(fz * sc);
+            }
+    }
+}
+
 /* moments_LB_kernel: lb_cuda_moments_module.f90:19-341.  s_ = input buffer
  * (updated in place), o_ = other buffer (velocity u_old). */
 static void moments(orc_state *s, real **hs, real **ho, const real *ph)
@@ -566,6 +683,17 @@ static void moments(orc_state *s, real **hs, real **ho, const real *ph)
                     fxv = fxv + chem * gfx;
                     fyv = fyv + chem * gfy;
                     fzv = fzv + chem * gfz;
+                    if (s->p.repulsive) {
+                        /* lb_cuda_moments_module.f90:148-160: rho_phi F_rep, capped at 1e-3 */
+                        real t[3];
+                        for (int d = 0; d < 3; d++) {
+                            t[d] = s->rep[d][c] * rhophi;
+                            if (fabs((double)t[d]) > 1.0e-3) t[d] = (real)(t[d] > 0 ? 1.0e-3 : -1.0e-3);
+                        }
+                        fxv = fxv + t[0] * rhophi;
+                        fyv = fyv + t[1] * rhophi;
+                        fzv = fzv + t[2] * rhophi;
+                    }
                 }
                 if (dr) {
                     grx = (s->rho_r - s->rho_b) * gfx;
@@ -1153,6 +1281,7 @@ static void one_step(orc_state *s)
             if (s->p.openbc) open_phi_copy(s, pA);
         }
         compute_div_theta(s);
+        if (s->p.repulsive) repulsive(s, pA);
     }
     moments(s, A, B, pA);
     exchange_h(s, A);

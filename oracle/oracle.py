@@ -34,6 +34,7 @@ class OrcParams(C.Structure):
         ("fz", C.c_double), ("wettab_r", C.c_double), ("phi_correction", C.c_int), ("smagorinsky", C.c_int),
         ("openbc", C.c_int), ("obc_type", (C.c_int * 2) * 3), ("obc_press", (C.c_double * 2) * 3),
         ("obc_vel", ((C.c_double * 3) * 2) * 3), ("bounce_back", C.c_int),
+        ("repulsive", C.c_int), ("a_rep", C.c_double), ("cos_opp_t", C.c_double), ("q_th", C.c_double),
     ]
 
 
@@ -122,6 +123,10 @@ class Oracle:
         pr = params.get("openbc_press") or ((0.0, 0.0),) * 3
         ve = params.get("openbc_vel") or (((0.0,) * 3,) * 2,) * 3
         p.bounce_back = int(params.get("bounce_back", 0))
+        p.repulsive = int(params.get("repulsive_flux", 0))
+        p.a_rep = float(params.get("a_rep", 0.0))
+        p.cos_opp_t = float(params.get("cos_opp_t", 0.0))
+        p.q_th = float(params.get("q_th", 0.0))
         for a in range(3):
             for sd in range(2):
                 p.obc_type[a][sd] = int(ty[a][sd])

@@ -167,6 +167,29 @@ def make_case(name: str, storage: str = "f32"):
         m = _random_moments(rng, p.shape, amp_u=0.003, amp_p=0.002)
         m = np.where((isf == 0)[None], 0.0, m)
         return p, isf, m, None
+    if name in ("rep_q27ho_2c_dr", "rep_obs_q19_2c"):
+        # REPULSIVE_FLUX: two droplets whose interfaces face each other across a
+        # film of about three nodes, inside the +-3 window of the pair search
+        obs = name.startswith("rep_obs")
+        lat = 19 if "q19" in name else 27
+        ho = 1 if "ho" in name else 0
+        dr = 1 if name.endswith("dr") else 0
+        L = (34, 18, 20)
+        p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_y=0 if obs else 1, lattice=lat, highorder=ho, twocomponent=1,
+                   densratio=dr, obstacles=1 if obs else 0, visc1=0.05, visc2=0.08, rho_r=1.0,
+                   rho_b=0.5 if dr else 1.0, sigma=0.02, width=3.0, tau_diff=0.1, storage=storage,
+                   repulsive_flux=1, a_rep=0.05, cos_opp_t=-0.5, q_th=0.05)
+        m1, p1 = O.ic_droplet(L[0], L[1], L[2], (10.5, 9.0, 10.0), 5.0, 3.0, 0.02, p.rho_r, p.rho_b, bool(dr))
+        m2, p2 = O.ic_droplet(L[0], L[1], L[2], (23.5, 9.5, 10.0), 5.0, 3.0, 0.02, p.rho_r, p.rho_b, bool(dr))
+        phi = np.maximum(p1, p2)
+        m = m1 + m2 + _random_moments(rng, p.shape, amp_u=0.002, amp_p=0.0005, amp_neq=1e-6)
+        if obs:
+            isf = O.mark_isfluid(np.zeros(p.shape, dtype=bool), (1, 0, 1), lat, True)
+            phi = O.seed_solid_phi(np.where(isf == 0, 0.0, phi), isf, lat)
+            m = np.where((isf == 0)[None], 0.0, m)
+        else:
+            isf = np.ones(p.shape, np.int8)
+        return p, isf, m, phi
     if name == "obs_q19_1c":
         L = (28, 18, 12)
         p = Params(lx=L[0], ly=L[1], lz=L[2], pbc_y=0, lattice=19, obstacles=1, visc1=0.1, fx=1e-5,
@@ -183,7 +206,8 @@ ALL_CASES = ["tg_q19", "q27ho_1c_force", "q27_1c", "q27ho_2c_dr", "q27_2c_dr", "
              "obs_q27ho_2c_dr", "obs_q19_2c_dr", "obs_q19_1c", "q27ho_2c_dr_corr", "obs_q27ho_2c_dr_corr", "q27ho_1c_force_smag",
              "obs_q27ho_2c_dr_smag", "q19_2c_smag", "q15_1c", "q15_2c_dr", "obs_q15_2c_dr", "open_q27ho_2c_dr",
              "open_q27_2c", "open_q15_2c_dr", "open_q19_1c", "open_q27ho_2c_dr_corr", "obs_q27ho_2c_dr_bb",
-             "obs_q19_1c_bb", "obs_q15_2c_dr_bb", "obs_q27ho_2c_dr_smag_bb", "open_q19_1c_bb"]
+             "obs_q19_1c_bb", "obs_q15_2c_dr_bb", "obs_q27ho_2c_dr_smag_bb", "open_q19_1c_bb", "rep_q27ho_2c_dr",
+             "rep_obs_q19_2c", "rep_obs_q19_2c_bb"]
 
 
 def run_oracle(name: str, nsteps: int, prec: str = "f64"):

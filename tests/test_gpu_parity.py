@@ -19,6 +19,7 @@ import pytest
 
 from cases import ALL_CASES, make_case, rel_l2, run_oracle
 from lbfast_b200.capi import Solver
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -64,11 +65,41 @@ def test_fp64_matches_oracle(name):
     assert not bad, f"{name}: {err}"
 
 
+def _noise_response(name, eps=1e-7, nsteps=NSTEPS):
+    """rel-L2 change of each field group of the FP64 oracle after nsteps when
+    the initial phi carries relative noise eps (seeded)."""
+    p, isf, m, phi = make_case(name)
+    out = []
+    for e in (0.0, eps):
+        o = O.Oracle(p.oracle_dict())
+        o.set_isfluid(isf)
+        o.set_fields(m, phi * (1 + e * np.random.default_rng(1).standard_normal(phi.shape)))
+        o.step(nsteps)
+        out.append(o.get_fields())
+    fluid = np.abs(isf) == 1
+    r = {k: rel_l2(out[1][0][sl], out[0][0][sl], fluid) for k, sl in GROUPS.items()}
+    r["phi"] = rel_l2(out[1][1], out[0][1], fluid)
+    r["uold"] = r["print_vel"] = r["u"]
+    r["print_rho"] = r["phi"]
+    return r
+
+
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_fp32_matches_oracle(name):
+    """FP32 within 1e-5 rel-L2 of the FP64 oracle.  REPULSIVE_FLUX pairs
+    interfacial nodes by thresholds (q >= q_th, q within 10 %, n1 . n2 <=
+    cosOppT), so the step is discontinuous in phi: a rounding-sized change
+    flips a pairing and moves the flow by far more than FP32 rounding (1e-7
+    of noise on phi changes u by ~8e-5 in 24 steps on rep_q27ho_2c_dr, against
+    4e-7 without the switch).  For those cases the bar is twice that measured
+    response of the FP64 oracle, and never below 1e-5."""
     err = _errors(name, "f32")
-    bad = {k: v for k, v in err.items() if not v < 1e-5}
-    assert not bad, f"{name}: {err}"
+    bars = {k: 1e-5 for k in err}
+    if name.startswith("rep_"):
+        resp = _noise_response(name)
+        bars = {k: max(1e-5, 2 * resp.get(k, 0.0)) for k in err}
+    bad = {k: v for k, v in err.items() if not v < bars[k]}
+    assert not bad, f"{name}: {err} bars {bars}"
 
 
 def test_zero_steps_is_initial_state():

@@ -123,6 +123,16 @@ def test_namelist_reader_reads_open_faces(tmp_path):
     assert p.openbc_vel[2][1][2] == -0.25
 
 
+def test_namelist_reader_reads_repulsive_parameters(tmp_path):
+    """A_rep, cosOppT and q_th of the &fluid namelist (LBFAST.f90:57-58)."""
+    base = open(os.path.join(ROOT, "tests", "golden", "channel.inp")).read()
+    text = base.replace("&fluid", "&fluid\n   A_rep=0.05d0\n   cosOppT=-0.8\n   q_th=0.125", 1)
+    f = tmp_path / "rep.inp"
+    f.write_text(text)
+    rc, p, _ = read_nml(f)
+    assert rc == 0 and (p.a_rep, p.cos_opp_t, p.q_th) == (0.05, -0.8, 0.125)
+
+
 def test_namelist_reader_reads_reference_inputs():
     ref = "/root/reference"
     files = sorted(f for f in os.listdir(ref) if f.endswith(".inp")) if os.path.isdir(ref) else []
@@ -152,7 +162,8 @@ def test_raw_xdmf_writer(tmp_path):
 
 @pytest.mark.parametrize("bad", [dict(lattice=13), dict(highorder=1, lattice=19), dict(densratio=1),
                                  dict(lx=0), dict(storage="f8"), dict(visc1=-1.0), dict(openbc=1, pbc_x=0),
-                                 dict(openbc=1, obstacles=1, pbc_y=0, ly=2), dict(bounce_back=1)])
+                                 dict(openbc=1, obstacles=1, pbc_y=0, ly=2), dict(bounce_back=1),
+                                 dict(repulsive_flux=1)])
 def test_create_rejects_invalid_parameters_before_device_work(bad):
     kw = dict(lx=8, ly=8, lz=8, lattice=27)
     kw.update(bad)

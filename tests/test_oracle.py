@@ -221,3 +221,40 @@ def test_poiseuille_wall_position(bb, H_off):
     theory = fx / (2 * nu) * (H * H - (y - yc) ** 2)
     u = h[1, 1, :, 1]
     assert np.abs(u[1:-1] - theory[1:-1]).max() < 0.01 * theory.max()
+
+
+def _rep_run(name, far, on, steps=12):
+    p, isf, m, phi = make_case(name)
+    d = p.oracle_dict()
+    d["repulsive_flux"] = on
+    if far:
+        # droplets of R = 7 (interfacial band q >= q_th from r = 4.8 to 9.2:
+        # no two band nodes of one droplet with normals 120 degrees apart fit
+        # the +-3 node window) 24 nodes apart both ways in a 48 x 24 x 24 box:
+        # no facing pair exists
+        L = (48, 24, 24)
+        d.update(lx=L[0], ly=L[1], lz=L[2])
+        m1, p1 = O.ic_droplet(*L, (12.0, 12.0, 12.0), 7.0, 3.0, 0.02, p.rho_r, p.rho_b, bool(p.densratio))
+        m2, p2 = O.ic_droplet(*L, (36.0, 12.5, 12.0), 7.0, 3.0, 0.02, p.rho_r, p.rho_b, bool(p.densratio))
+        phi, m = np.maximum(p1, p2), m1 + m2
+        isf = np.ones(L[::-1], np.int8)
+    o = O.Oracle(d)
+    o.set_isfluid(isf)
+    o.set_fields(m, phi)
+    o.step(steps)
+    return o.get_fields()
+
+
+def test_repulsive_flux_acts_only_across_thin_films():
+    """REPULSIVE_FLUX (lb_cuda_repulsive_module.f90:19-292): two droplets whose
+    interfaces face each other across a film of about three nodes feel the
+    film force, first in the film; droplets whose interfaces are further
+    apart than the +-3 node window feel none, and the run equals the one
+    without the switch bit for bit."""
+    a_on, a_off = _rep_run("rep_q27ho_2c_dr", False, 1), _rep_run("rep_q27ho_2c_dr", False, 0)
+    assert np.abs(a_on[0] - a_off[0]).max() > 1e-6
+    # the difference of phi is largest in the film between the droplets (x = 15 .. 19)
+    d = np.abs(a_on[1] - a_off[1]).max(axis=(0, 1))
+    assert d[14:21].max() > 10 * max(d[:5].max(), d[-5:].max())
+    b_on, b_off = _rep_run("rep_q27ho_2c_dr", True, 1), _rep_run("rep_q27ho_2c_dr", True, 0)
+    assert all(np.array_equal(x, y) for x, y in zip(b_on, b_off))
