@@ -56,9 +56,11 @@ constexpr double SMAG_C = (double)(0.053f * 18.0f);
 // fields staged per collision node: 10 moments (+3 u_old with a density ratio)
 constexpr int NSTAGE = 13;
 
-// FP32 storage is prefetched with cp.async; 16-bit and FP64 storage are read at
-// the point of use (FP64 leaves no shared memory for a staging area)
-template <typename S> constexpr bool staged() { return sizeof(S) == 4; }
+// FP32 storage is prefetched with cp.async into a staging area on tiles of 16
+// rows; 16-bit and FP64 storage, and tiles of 8 rows, read at the point of use
+// (FP64 leaves no shared memory for a staging area; without it an 8-row tile
+// needs 99 KB and two CTAs share an SM)
+template <typename S, int TYV> constexpr bool staged() { return sizeof(S) == 4 && TYV > 8; }
 
 // ring slots of the separable phase-field stencils (see step_body)
 constexpr int SXY_SLOTS = 5, GXY_SLOTS = 3, TH_SLOTS = 2, GT_SLOTS = 3, H_SLOTS = 3;
@@ -74,7 +76,7 @@ template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t st
     if (TC)
         b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(SXY_SLOTS) * R2N + size_t(GXY_SLOTS) * 2 * R2N +
                           size_t(TH_SLOTS) * 3 * R2N + size_t(GT_SLOTS) * 3 * R1N + size_t(H_SLOTS) * 3 * R1N);
-    if (staged<S>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
+    if (staged<S, TYV>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
     return b;
 }
 
@@ -90,7 +92,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
     using CP = Codec<SP>;
-    constexpr bool STG = staged<S>();
+    constexpr bool STG = staged<S, TYV>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // post-collision populations of plane q, by (cx, cy) group g = 3 (cy+1) + (cx+1):
     // the output nodes that read one group of a node read all three cz of it
