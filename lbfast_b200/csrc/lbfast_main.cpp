@@ -3,6 +3,7 @@
 //
 //   lbfast [-DLATTICE=15|19|27] [-DHIGHORDER] [-DTWOCOMPONENT] [-DDENSRATIO]
 //          [-DINTERNAL_OBSTACLES] [-DWETTABILITY] [-DPRINTPHI] [-DWRITEPRESS] [-DSMAGORINSKI] [-DBOUNCE_BACK]
+//          [-DREPULSIVE_FLUX]
 //          [-DTAYLORGREEN|-DLAPLACE|-DLAMBTEST] [--storage=f32|f16|bf16|f64]
 //          input.inp
 //
@@ -34,6 +35,7 @@ struct Flags {
     int lattice = 27;
     bool highorder = false, twocomponent = false, densratio = false, obstacles = false;
     bool printphi = false, writepress = false, wettability = false, smagorinsky = false, bounce_back = false;
+    bool repulsive = false;
     bool taylorgreen = false, laplace = false, lambtest = false;
     int storage = LBF_STORE_F32;
     std::string input;
@@ -74,6 +76,7 @@ Flags parse_flags(int argc, char** argv) {
         else if (a == "-DWETTABILITY") fl.wettability = true;
         else if (a == "-DSMAGORINSKI") fl.smagorinsky = true;
         else if (a == "-DBOUNCE_BACK") fl.bounce_back = true;
+        else if (a == "-DREPULSIVE_FLUX") fl.repulsive = true;
         else if (a == "-DPRINTPHI") fl.printphi = true;
         else if (a == "-DWRITEPRESS") fl.writepress = true;
         else if (a == "-DTAYLORGREEN") fl.taylorgreen = true;
@@ -118,6 +121,7 @@ int main(int argc, char** argv) {
     p.printphi = fl.printphi;
     p.smagorinsky = fl.smagorinsky;
     p.bounce_back = fl.bounce_back;
+    p.repulsive_flux = fl.repulsive;
     p.visc2 = 0.0;
     p.wettab_r = 90.0;
     lbf_run run;

@@ -41,7 +41,7 @@ def _fp16_errors(name, n=100):
     return err
 
 
-@pytest.mark.parametrize("name", ["q27ho_2c_dr", "obs_q27ho_2c_dr"])
+@pytest.mark.parametrize("name", ["q27ho_2c_dr", "obs_q27ho_2c_dr", "open_q27ho_2c_dr", "obs_q27ho_2c_dr_bb"])
 def test_fp16_storage_two_component_within_1e3(name):
     """16-bit storage (u, u_old and Pi - u u in FP16, one power-of-two scale per
     field group; P and phi in FP32; FP32 arithmetic) after 100 steps against the

@@ -16,10 +16,12 @@ import lbfast_b200 as L
 pytestmark = pytest.mark.gpu
 
 # (case, storage, nsteps): three kernel classes, ragged boxes, wetting on
-# obstacles, open faces, step counts that are not multiples of the chunk
+# obstacles, open faces, bounce-back, the repulsive-flux kernel class, step
+# counts that are not multiples of the chunk
 MIX = [("q27_2c_dr", "f16", 23), ("q27ho_2c_dr", "f32", 17), ("tg_q19", "f32", 30), ("obs_q27ho_2c_dr", "f32", 12),
        ("q27ho_2c_dr_corr", "f32", 15), ("q19_2c_dr", "f16", 9), ("q27_2c_dr", "f32", 40),
-       ("open_q27ho_2c_dr_corr", "f32", 14), ("open_q19_1c", "f16", 11)]
+       ("open_q27ho_2c_dr_corr", "f32", 14), ("open_q19_1c", "f16", 11), ("rep_q27ho_2c_dr", "f32", 10),
+       ("obs_q19_1c_bb", "f16", 13)]
 
 
 def _alone(case, storage, n, **kw):
@@ -64,7 +66,7 @@ def test_graph_and_direct_launches_agree(alone):
     assert _same(_alone(c, st, n, chunk=8, use_graph=True), alone[i])
 
 
-@pytest.mark.parametrize("i", [0, 1, 2, 3, 4, 7, 8])
+@pytest.mark.parametrize("i", [0, 1, 2, 3, 4, 7, 8, 9, 10])
 def test_server_equals_single_box_entry_point(alone, i):
     """The server's result equals lbf_step's on the same inputs."""
     c, st, n = MIX[i]
