@@ -51,26 +51,96 @@ B_LUP = {"f32": 112, "f16": 64, "bf16": 64, "f64": 224}  # algorithmic bytes per
 NCU_TRAFFIC = {("f32", 256): 1845157888}
 
 
-def workload(storage: str = "f32", L: int = LBOX):
+CHANNEL = (512, 256, 256)  # the two-component channel with obstacles (lx, ly, lz)
+
+
+def channel_geometry(lx=CHANNEL[0], ly=CHANNEL[1], lz=CHANNEL[2]):
+    """isfluid and phi of the channel: walls at y = 0 and ly-1 (pbc 1, 0, 1),
+    64 seeded solid spheres of radius U[6, 14] kept clear of the periodic faces
+    (seed 12345), phi from 32 seeded blobs of radius U[8, 24] with a width-4
+    tanh profile (seed 67890), solid-node phi seeded from fluid neighbours."""
+    import numpy as np
+
     import lbfast_b200 as lbf
+    rng = np.random.default_rng(12345)
+    solid = np.zeros((lz, ly, lx), dtype=bool)
+    for _ in range(64):
+        r = rng.uniform(6.0, 14.0)
+        lo = r + 1.5
+        c = [rng.uniform(lo, n - 1 - lo) for n in (lx, ly, lz)]
+        z0, z1 = int(c[2] - r) - 1, int(c[2] + r) + 2
+        y0, y1 = int(c[1] - r) - 1, int(c[1] + r) + 2
+        x0, x1 = int(c[0] - r) - 1, int(c[0] + r) + 2
+        z, y, x = np.ogrid[z0:z1, y0:y1, x0:x1]
+        solid[z0:z1, y0:y1, x0:x1] |= (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r
+    isf = lbf.mark_isfluid(np.where(solid, 0, 1).astype(np.int8), (1, 0, 1), 27, True)
+    rng = np.random.default_rng(67890)
+    phi = np.zeros((lz, ly, lx))
+    for _ in range(32):
+        r = rng.uniform(8.0, 24.0)
+        c = rng.uniform(0, 1, 3) * np.array([lx, ly, lz])
+        h = int(r + 10)
+        zi = (np.arange(int(c[2]) - h, int(c[2]) + h + 1)) % lz
+        yi = np.clip(np.arange(int(c[1]) - h, int(c[1]) + h + 1), 0, ly - 1)
+        xi = (np.arange(int(c[0]) - h, int(c[0]) + h + 1)) % lx
+        dz = np.arange(int(c[2]) - h, int(c[2]) + h + 1)[:, None, None] - c[2]
+        dy = np.arange(int(c[1]) - h, int(c[1]) + h + 1)[None, :, None] - c[1]
+        dx = np.arange(int(c[0]) - h, int(c[0]) + h + 1)[None, None, :] - c[0]
+        blob = 0.5 * (1.0 - np.tanh((np.sqrt(dx * dx + dy * dy + dz * dz) - r) / 2.0))
+        sub = phi[np.ix_(zi, yi, xi)]
+        phi[np.ix_(zi, yi, xi)] = np.maximum(sub, blob)
+    phi = np.where(isf == 0, 0.0, phi)
+    phi = lbf.seed_solid_phi(phi, isf, 27)
+    return isf, phi
+
+
+def workload(storage: str = "f32", L: int = LBOX, kind: str = "laplace"):
+    """(Params, moments, phi, isfluid or None) of the Laplace droplet (L^3,
+    the headline) or of the channel with obstacles (512 x 256 x 256: walls,
+    spheres and wetting at 90 degrees, body force 1e-6, the twopoiseuille.inp
+    fluid parameters)."""
+    import numpy as np
+
+    import lbfast_b200 as lbf
+    if kind == "channel":
+        lx, ly, lz = CHANNEL
+        p = lbf.Params(lx=lx, ly=ly, lz=lz, pbc_y=0, lattice=27, highorder=1, twocomponent=1, densratio=1,
+                       obstacles=1, visc1=0.05, visc2=0.4, rho_r=0.5, rho_b=1.5, sigma=0.0, width=4.0,
+                       tau_diff=0.1, fx=1e-6, wettab_r=90.0, printphi=1, storage=storage)
+        isf, phi = channel_geometry(lx, ly, lz)
+        return p, np.zeros((10, lz, ly, lx)), phi, isf
     p = lbf.Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1,
                    visc1=0.1, visc2=0.1, rho_r=RHO_R, rho_b=RHO_B, sigma=0.03, width=3.0, tau_diff=0.1,
                    printphi=1, storage=storage)
     R = 40.0 * L / 256
     m, phi = lbf.ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, RHO_R, RHO_B, True)
-    return p, m, phi
+    return p, m, phi, None
 
 
-def config_dict(storage, L=LBOX):
-    return {"workload": f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO "
-                        f"(rho_r/rho_b = {RHO_R:g}/{RHO_B:g}), "
-                        f"R={int(40 * L / 256)}, width 3, sigma 0.03",
-            "box": [L, L, L], "lattice": "D3Q27", "highorder": True, "twocomponent": True, "densratio": True,
-            "storage": storage, "bytes_per_lup": B_LUP[storage],
-            "l2_policy": ("state (%.2f GB) larger than the 126 MB L2; no flush" % (L ** 3 * B_LUP[storage] / 1e9)
-                          if L ** 3 * B_LUP[storage] / 2 > 126e6 else
-                          "state (%.3f GB) fits in the 126 MB L2: not a valid headline size" %
-                          (L ** 3 * B_LUP[storage] / 1e9))}
+def box_of(kind, L=LBOX):
+    return list(CHANNEL) if kind == "channel" else [L, L, L]
+
+
+def bytes_per_lup(storage, kind):
+    return B_LUP[storage] + (1 if kind == "channel" else 0)  # + the isfluid byte with obstacles
+
+
+def config_dict(storage, L=LBOX, kind="laplace"):
+    box = box_of(kind, L)
+    n = box[0] * box[1] * box[2]
+    b = bytes_per_lup(storage, kind)
+    if kind == "channel":
+        text = ("two-component channel with obstacles 512x256x256, D3Q27 HIGHORDER DENSRATIO (rho 0.5/1.5, "
+                "nu 0.05/0.4), walls at y = 0 and 255, 64 seeded spheres R U[6,14], seeded phi blobs, "
+                "wetting 90 degrees, fx 1e-6, fluids at rest")
+    else:
+        text = (f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO "
+                f"(rho_r/rho_b = {RHO_R:g}/{RHO_B:g}), R={int(40 * L / 256)}, width 3, sigma 0.03")
+    return {"workload": text, "box": box, "lattice": "D3Q27", "highorder": True, "twocomponent": True,
+            "densratio": True, "obstacles": kind == "channel", "storage": storage, "bytes_per_lup": b,
+            "l2_policy": ("state (%.2f GB) larger than the 126 MB L2; no flush" % (n * b / 1e9)
+                          if n * b / 2 > 126e6 else
+                          "state (%.3f GB) fits in the 126 MB L2: not a valid headline size" % (n * b / 1e9))}
 
 
 class ClockSampler:
@@ -135,11 +205,13 @@ def run_ours(args, rank, local, world):
     import lbfast_b200 as lbf
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    p, m, phi = workload(args.storage, args.box)
+    p, m, phi, isf = workload(args.storage, args.box, args.workload)
     p.tile_y, p.zseg = args.tile, args.zseg
     N = p.lx * p.ly * p.lz
     s = lbf.Solver(p)
     s.set_stream(stream.cuda_stream)
+    if isf is not None:
+        s.set_isfluid(isf)
     s.set_fields(m, phi)
     s.step(args.warmup)  # the first step runs the autotuner (schedule: z segments or persistent)
     s.sync()
@@ -158,8 +230,9 @@ def run_ours(args, rank, local, world):
     clocks = clk.summary()
     ms_step = ms / args.steps
     value = weak_scaling_value(N, args.steps, ms, world)
-    # the step kernel is the only launch per step: its average duration is the step time
-    bytes_launch = B_LUP[args.storage] * N
+    # the step kernel is the only launch per step (with obstacles the small
+    # wetting kernel precedes it): the step time bounds its average duration
+    bytes_launch = bytes_per_lup(args.storage, args.workload) * N
     achieved = bytes_launch / (ms_step * 1e-3) / 1e9
     try:
         ok = bool(np.all(np.isfinite(s.reduce())))
@@ -177,6 +250,8 @@ def run_ours(args, rank, local, world):
     press = torch.empty((p.lz, p.ly, p.lx), dtype=torch.float32, pin_memory=True).numpy()
     s = lbf.Solver(p)
     s.set_stream(stream.cuda_stream)
+    if isf is not None:
+        s.set_isfluid(isf)
     import ctypes as C
     lib = lbf.load()
     fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
@@ -344,15 +419,15 @@ def run_serving(n: int, nsteps: int, seed: int = 7):
     }
 
 
-def cpu_baseline(storage: str, L: int, nsteps: int, threads: int):
+def cpu_baseline(storage: str, L: int, nsteps: int, threads: int, kind: str = "laplace"):
     """The oracle (C restatement of the reference, FP32 build stand-in) on the
     host cores: `nsteps` steps of the same box."""
     import numpy as np
     from oracle import oracle as O
-    p, m, phi = workload(storage, L)
+    p, m, phi, isf = workload(storage, L, kind)
     O.set_threads(threads)
     o = O.Oracle(p.oracle_dict(), "f32")
-    o.set_isfluid(np.ones(p.shape, np.int8))
+    o.set_isfluid(isf if isf is not None else np.ones(p.shape, np.int8))
     o.set_fields(m, phi)
     o.step(0)
     t0 = time.perf_counter()
@@ -368,7 +443,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
-    ap.add_argument("--box", type=int, default=LBOX)
+    ap.add_argument("--box", type=int, default=LBOX, help="edge of the Laplace box")
+    ap.add_argument("--workload", default="laplace", choices=["laplace", "channel"],
+                    help="laplace: the droplet box (headline); channel: 512x256x256 with obstacles")
     ap.add_argument("--tile", type=int, default=0, help="kernel tile rows (8 or 16); 0: autotuned")
     ap.add_argument("--zseg", type=int, default=0, help="planes per z segment; 0: autotuned / automatic")
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU baseline sample")
@@ -387,15 +464,15 @@ def main():
             return
         # each timed step of the reference arm is one full oracle step of the box
         for _ in range(min(args.warmup, 1)):
-            cpu_baseline(args.storage, args.box, 1, threads)
+            cpu_baseline(args.storage, args.box, 1, threads, args.workload)
         k = max(1, min(args.steps, 20))
-        mlups, dt = cpu_baseline(args.storage, args.box, k, threads)
+        mlups, dt = cpu_baseline(args.storage, args.box, k, threads, args.workload)
         line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": k, "warmup": min(args.warmup, 1), "ms_per_step": dt / k * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_dict(args.storage, args.box),
+                "config": config_dict(args.storage, args.box, args.workload),
                 "cpu_baseline": {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{k} steps of the {args.box}^3 box, FP32 C restatement of the "
+                                 "sample": f"{k} steps of the {box_of(args.workload, args.box)} box, FP32 C restatement of the "
                                            f"reference kernels (oracle/lbf_oracle.c), OpenMP over z"},
                 "e2e": {"value": mlups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -413,9 +490,9 @@ def main():
     r = run_ours(args, rank, local, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        mlups, dt = cpu_baseline(args.storage, args.box, args.cpu_steps, threads)
+        mlups, dt = cpu_baseline(args.storage, args.box, args.cpu_steps, threads, args.workload)
         cpu = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of the same {args.box}^3 box ({dt:.1f} s), FP32 C restatement of "
+               "sample": f"{args.cpu_steps} steps of the same {box_of(args.workload, args.box)} box ({dt:.1f} s), FP32 C restatement of "
                          f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
     serving = None
     if rank == 0 and world == 1 and args.serve_solves > 0:
@@ -423,16 +500,19 @@ def main():
     if rank != 0:
         shutdown(world)
         return
-    traffic = NCU_TRAFFIC.get((args.storage, args.box))
+    traffic = NCU_TRAFFIC.get((args.storage, args.box)) if args.workload == "laplace" else None
+    nbox = box_of(args.workload, args.box)
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64", "data": "synthetic",
-        "config": dict(config_dict(args.storage, args.box), parallelism=f"replicas x{world}"),
+        "config": dict(config_dict(args.storage, args.box, args.workload), parallelism=f"replicas x{world}"),
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": peak, "unit": "GB/s",
                      "frac": r["achieved"] / peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "lbf::stream_kernel<27,HO,TC>", "launch": r["tuning"], "bytes_per_launch": B_LUP[args.storage] * args.box ** 3},
-        "e2e": r["e2e"], "gpu_launches": args.steps, "clocks": r["clocks"], "cpu_baseline": cpu,
+                     "kernel": "lbf::stream_kernel<27,HO,TC>", "launch": r["tuning"],
+                     "bytes_per_launch": bytes_per_lup(args.storage, args.workload) * nbox[0] * nbox[1] * nbox[2]},
+        "e2e": r["e2e"], "gpu_launches": args.steps * (2 if args.workload == "channel" else 1), "clocks": r["clocks"],
+        "cpu_baseline": cpu,
         "finite": r["finite"], "serving": serving,
     }
     print(json.dumps(line))

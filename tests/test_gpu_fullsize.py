@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import lbfast_b200 as L
+from bench import channel_geometry
 from cases import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -24,36 +25,7 @@ NSTEPS = 200
 
 
 def _geometry():
-    rng = np.random.default_rng(12345)
-    solid = np.zeros((LZ, LY, LX), dtype=bool)
-    for _ in range(64):
-        r = rng.uniform(6.0, 14.0)
-        lo = r + 1.5
-        c = [rng.uniform(lo, n - 1 - lo) for n in (LX, LY, LZ)]
-        z0, z1 = int(c[2] - r) - 1, int(c[2] + r) + 2
-        y0, y1 = int(c[1] - r) - 1, int(c[1] + r) + 2
-        x0, x1 = int(c[0] - r) - 1, int(c[0] + r) + 2
-        z, y, x = np.ogrid[z0:z1, y0:y1, x0:x1]
-        solid[z0:z1, y0:y1, x0:x1] |= (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r
-    isf = L.mark_isfluid(np.where(solid, 0, 1).astype(np.int8), (1, 0, 1), 27, True)
-    rng = np.random.default_rng(67890)
-    phi = np.zeros((LZ, LY, LX))
-    for _ in range(32):
-        r = rng.uniform(8.0, 24.0)
-        c = rng.uniform(0, 1, 3) * np.array([LX, LY, LZ])
-        h = int(r + 10)
-        zi = (np.arange(int(c[2]) - h, int(c[2]) + h + 1)) % LZ
-        yi = np.clip(np.arange(int(c[1]) - h, int(c[1]) + h + 1), 0, LY - 1)
-        xi = (np.arange(int(c[0]) - h, int(c[0]) + h + 1)) % LX
-        dz = np.arange(int(c[2]) - h, int(c[2]) + h + 1)[:, None, None] - c[2]
-        dy = np.arange(int(c[1]) - h, int(c[1]) + h + 1)[None, :, None] - c[1]
-        dx = np.arange(int(c[0]) - h, int(c[0]) + h + 1)[None, None, :] - c[0]
-        blob = 0.5 * (1.0 - np.tanh((np.sqrt(dx * dx + dy * dy + dz * dz) - r) / 2.0))
-        sub = phi[np.ix_(zi, yi, xi)]
-        phi[np.ix_(zi, yi, xi)] = np.maximum(sub, blob)
-    phi = np.where(isf == 0, 0.0, phi)
-    phi = L.seed_solid_phi(phi, isf, 27)
-    return isf, phi
+    return channel_geometry(LX, LY, LZ)
 
 
 @pytest.fixture(scope="module")
