@@ -142,7 +142,7 @@ int autotune(lbf_handle* h) {
         if (it != g_tune_cache.end()) {
             h->tile_y = it->second.first;
             h->zseg = it->second.second;
-            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->tile_y);
+            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, h->tile_y);
             return LBF_OK;
         }
     }
@@ -170,7 +170,7 @@ int autotune(lbf_handle* h) {
     std::pair<int, int> pick(h->tile_y, h->zseg);
     int rc = LBF_OK;
     for (const auto& c : cand) {
-        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), c.first);
+        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, c.first);
         if (!L) continue;
         lbf::StepArgs a;
         const int zs0 = h->zseg;
@@ -198,7 +198,7 @@ int autotune(lbf_handle* h) {
     if (rc) return rc;
     h->tile_y = pick.first;
     h->zseg = pick.second;
-    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->tile_y);
+    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, h->tile_y);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = pick;
     return LBF_OK;
@@ -365,7 +365,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     // 16 rows do not fit in shared memory); tile_y = 0 also tunes the schedule
     h->tile_y = p->tile_y ? p->tile_y : (lbf::tile_available(p->storage, 16) ? 16 : 8);
     h->tuned = p->tile_y != 0;
-    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, lbf::kernel_tc(*p), h->tile_y);
+    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, lbf::kernel_tc(*p), p->obstacles, h->tile_y);
     if (!h->launcher) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");

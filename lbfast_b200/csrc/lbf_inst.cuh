@@ -40,12 +40,12 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.rep = static_cast<const R*>(a.rep);
 }
 
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false, bool OBS = true>
 cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     static bool attr_set = false;
     const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV, REP>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
@@ -54,48 +54,48 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     make_params(a, p);
     if (a.zseg > 0) {
         dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
-        stream_kernel<LAT, HO, TC, S, R, TYV, REP><<<grid, TX * TYV, smem, st>>>(p);
+        stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<grid, TX * TYV, smem, st>>>(p);
         return cudaGetLastError();
     }
     static int resident = 0;  // CTAs per SM at this shared-memory size
     if (!resident) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel<LAT, HO, TC, S, R, TYV, REP>,
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS>,
                                                                       TX * TYV, smem);
         if (e != cudaSuccess) return e;
         if (resident < 1) return cudaErrorInvalidConfiguration;
     }
     const long long W = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV) * a.nz;
     const int grid = persistent_grid(W, resident);
-    stream_kernel<LAT, HO, TC, S, R, TYV, REP><<<grid, TX * TYV, smem, st>>>(p);
+    stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<grid, TX * TYV, smem, st>>>(p);
     return cudaGetLastError();
 }
 
 // One launch advancing many boxes of one kernel class: d_boxes holds one
 // StepParams per box, d_work one (box, first column-plane, end column-plane)
 // per CTA.
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false>
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false, bool OBS = true>
 cudaError_t launch_stream_batched(const void* d_boxes, const int4* d_work, int nwork, cudaStream_t st) {
     static bool attr_set = false;
     const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
+        cudaError_t e = cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP, OBS>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (nwork <= 0) return cudaSuccess;
-    stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>
+    stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP, OBS>
         <<<nwork, TX * TYV, smem, st>>>(static_cast<const StepParams<S, R>*>(d_boxes), d_work);
     return cudaGetLastError();
 }
 
-template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false> int batched_resident() {
+template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false, bool OBS = true> int batched_resident() {
     static int resident = 0;
     if (!resident) {
         const size_t smem = stream_smem_bytes<LAT, TC, S, R, TYV>();
-        if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
+        if (cudaFuncSetAttribute(stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP, OBS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP>,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, stream_kernel_batched<LAT, HO, TC, S, R, TYV, REP, OBS>,
                                                           TX * TYV, smem) != cudaSuccess)
             resident = 1;
         resident = std::max(resident, 1);
@@ -108,48 +108,59 @@ template <typename S, typename R> void fill_params(const StepArgs& a, void* dst)
 }
 
 // the kernel classes of one storage type and tile height; tc: 0 one
-// component, 1 two components, 2 two components with REPULSIVE_FLUX
-template <int LAT, bool HO, typename S, typename R, int TYV> StepLauncher step_class(int tc) {
-    return tc == 2 ? &launch_stream<LAT, HO, true, S, R, TYV, true>
-                   : tc ? &launch_stream<LAT, HO, true, S, R, TYV> : &launch_stream<LAT, HO, false, S, R, TYV>;
+// component, 1 two components, 2 two components with REPULSIVE_FLUX; obs:
+// obstacles
+template <int LAT, bool HO, typename S, typename R, int TYV, bool OBS> StepLauncher step_class(int tc) {
+    return tc == 2 ? &launch_stream<LAT, HO, true, S, R, TYV, true, OBS>
+                   : tc ? &launch_stream<LAT, HO, true, S, R, TYV, false, OBS>
+                        : &launch_stream<LAT, HO, false, S, R, TYV, false, OBS>;
 }
-template <typename S, typename R, int TYV> StepLauncher step_table(int lat, int ho, int tc) {
-    if (lat == 15 && !ho) return step_class<15, false, S, R, TYV>(tc);
-    if (lat == 19 && !ho) return step_class<19, false, S, R, TYV>(tc);
-    if (lat == 27 && ho) return step_class<27, true, S, R, TYV>(tc);
-    if (lat == 27 && !ho) return step_class<27, false, S, R, TYV>(tc);
+template <int LAT, bool HO, typename S, typename R, int TYV> StepLauncher step_class(int tc, int obs) {
+    return obs ? step_class<LAT, HO, S, R, TYV, true>(tc) : step_class<LAT, HO, S, R, TYV, false>(tc);
+}
+template <typename S, typename R, int TYV> StepLauncher step_table(int lat, int ho, int tc, int obs) {
+    if (lat == 15 && !ho) return step_class<15, false, S, R, TYV>(tc, obs);
+    if (lat == 19 && !ho) return step_class<19, false, S, R, TYV>(tc, obs);
+    if (lat == 27 && ho) return step_class<27, true, S, R, TYV>(tc, obs);
+    if (lat == 27 && !ho) return step_class<27, false, S, R, TYV>(tc, obs);
     return nullptr;
 }
 
-template <int LAT, bool HO, typename S, typename R, int TYV> void batch_class(int tc, BatchOps& o) {
+template <int LAT, bool HO, typename S, typename R, int TYV, bool OBS> void batch_class(int tc, BatchOps& o) {
     if (tc == 2) {
-        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV, true>;
-        o.resident = &batched_resident<LAT, HO, true, S, R, TYV, true>;
+        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV, true, OBS>;
+        o.resident = &batched_resident<LAT, HO, true, S, R, TYV, true, OBS>;
     } else if (tc) {
-        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV>;
-        o.resident = &batched_resident<LAT, HO, true, S, R, TYV>;
+        o.launch = &launch_stream_batched<LAT, HO, true, S, R, TYV, false, OBS>;
+        o.resident = &batched_resident<LAT, HO, true, S, R, TYV, false, OBS>;
     } else {
-        o.launch = &launch_stream_batched<LAT, HO, false, S, R, TYV>;
-        o.resident = &batched_resident<LAT, HO, false, S, R, TYV>;
+        o.launch = &launch_stream_batched<LAT, HO, false, S, R, TYV, false, OBS>;
+        o.resident = &batched_resident<LAT, HO, false, S, R, TYV, false, OBS>;
     }
 }
-template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho, int tc) {
+template <int LAT, bool HO, typename S, typename R, int TYV> void batch_class(int tc, int obs, BatchOps& o) {
+    if (obs) batch_class<LAT, HO, S, R, TYV, true>(tc, o);
+    else batch_class<LAT, HO, S, R, TYV, false>(tc, o);
+}
+template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho, int tc, int obs) {
     BatchOps o;
     o.params_bytes = sizeof(StepParams<S, R>);
     o.fill = &fill_params<S, R>;
     o.tile_y = TYV;
     o.launch = nullptr;
     o.resident = nullptr;
-    if (lat == 15 && !ho) batch_class<15, false, S, R, TYV>(tc, o);
-    if (lat == 19 && !ho) batch_class<19, false, S, R, TYV>(tc, o);
-    if (lat == 27 && ho) batch_class<27, true, S, R, TYV>(tc, o);
-    if (lat == 27 && !ho) batch_class<27, false, S, R, TYV>(tc, o);
+    if (lat == 15 && !ho) batch_class<15, false, S, R, TYV>(tc, obs, o);
+    if (lat == 19 && !ho) batch_class<19, false, S, R, TYV>(tc, obs, o);
+    if (lat == 27 && ho) batch_class<27, true, S, R, TYV>(tc, obs, o);
+    if (lat == 27 && !ho) batch_class<27, false, S, R, TYV>(tc, obs, o);
     return o;
 }
 
 // instantiation unit of one storage type and tile height (lbf_inst_<storage>_t<rows>.cu)
 #define LBF_INSTANTIATE(NAME, S, R, TYV)                                                                  \
-    StepLauncher step_launcher_##NAME##_t##TYV(int lat, int ho, int tc) { return step_table<S, R, TYV>(lat, ho, tc); } \
-    BatchOps batch_ops_##NAME##_t##TYV(int lat, int ho, int tc) { return batch_table<S, R, TYV>(lat, ho, tc); }
+    StepLauncher step_launcher_##NAME##_t##TYV(int lat, int ho, int tc, int obs) {                        \
+        return step_table<S, R, TYV>(lat, ho, tc, obs);                                                   \
+    }                                                                                                     \
+    BatchOps batch_ops_##NAME##_t##TYV(int lat, int ho, int tc, int obs) { return batch_table<S, R, TYV>(lat, ho, tc, obs); }
 
 }  // namespace lbf

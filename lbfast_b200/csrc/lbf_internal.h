@@ -33,7 +33,7 @@ using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
 
 // Step launcher of one kernel class (lattice 19/27, HIGHORDER, TWOCOMPONENT)
 // for a storage type and tile height (8 or 16 rows); nullptr if not built.
-StepLauncher step_launcher(int storage, int lat, int ho, int tc, int tile_y);
+StepLauncher step_launcher(int storage, int lat, int ho, int tc, int obs, int tile_y);
 // kernel class argument `tc` of a run: 0 one component, 1 two components,
 // 2 two components with REPULSIVE_FLUX (its own compilation of the step)
 inline int kernel_tc(const lbf_params& p) { return p.twocomponent ? (p.repulsive_flux ? 2 : 1) : 0; }
@@ -55,7 +55,7 @@ struct BatchOps {
 // persistent launch over W column-planes (no share shorter than 8 planes)
 int resident_slots(int resident_per_sm);
 int persistent_grid(long long W, int resident_per_sm);
-BatchOps batch_ops(int storage, int lat, int ho, int tc, int tile_y);
+BatchOps batch_ops(int storage, int lat, int ho, int tc, int obs, int tile_y);
 // CTA tile width of the step kernel in nodes (the height is 8 or 16)
 constexpr int STEP_TILE_X = 32;
 

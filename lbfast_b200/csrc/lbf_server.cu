@@ -80,11 +80,12 @@ struct Solve {
 };
 
 struct ClassKey {
-    int lat, ho, tc, storage, tile;
+    int lat, ho, tc, obs, storage, tile;
     bool operator<(const ClassKey& o) const {
         if (lat != o.lat) return lat < o.lat;
         if (ho != o.ho) return ho < o.ho;
         if (tc != o.tc) return tc < o.tc;
+        if (obs != o.obs) return obs < o.obs;
         if (storage != o.storage) return storage < o.storage;
         return tile < o.tile;
     }
@@ -194,10 +195,11 @@ int rebuild(lbf_server* s) {
     drop_graph(s);
     for (auto& kv : s->batches) kv.second.members.clear();
     for (Solve* v : s->active) {
-        ClassKey k{v->p.lattice, v->p.highorder, lbf::kernel_tc(v->p), v->p.storage, solve_tile(v->p)};
+        ClassKey k{v->p.lattice, v->p.highorder, lbf::kernel_tc(v->p), v->p.obstacles ? 1 : 0, v->p.storage,
+                   solve_tile(v->p)};
         Batch& b = s->batches[k];
         if (!b.ops.launch) {
-            b.ops = lbf::batch_ops(k.storage, k.lat, k.ho, k.tc, k.tile);
+            b.ops = lbf::batch_ops(k.storage, k.lat, k.ho, k.tc, k.obs, k.tile);
             if (!b.ops.launch) return sfail(LBF_E_UNSUPPORTED, "no batched kernel for this class");
             // sets the kernel's shared-memory attribute outside any graph capture
             SRV_TRY(b.ops.launch(nullptr, nullptr, 0, s->stream));
