@@ -138,9 +138,12 @@ template <int LAT, bool HO, typename S, typename R, int TYV, bool OBS> void batc
         o.resident = &batched_resident<LAT, HO, false, S, R, TYV, false, OBS>;
     }
 }
-template <int LAT, bool HO, typename S, typename R, int TYV> void batch_class(int tc, int obs, BatchOps& o) {
-    if (obs) batch_class<LAT, HO, S, R, TYV, true>(tc, o);
-    else batch_class<LAT, HO, S, R, TYV, false>(tc, o);
+// The batched kernels keep obstacles a run-time flag (OBS = true for every
+// box): the obstacle-free compilation of the batched kernel, unlike the
+// single-box one, ran the droplet-ensemble server slower and erratically
+// (3.2-5.2 against a steady 5.5 solves/s, interleaved runs on one box).
+template <int LAT, bool HO, typename S, typename R, int TYV> void batch_class(int tc, int, BatchOps& o) {
+    batch_class<LAT, HO, S, R, TYV, true>(tc, o);
 }
 template <typename S, typename R, int TYV> BatchOps batch_table(int lat, int ho, int tc, int obs) {
     BatchOps o;
