@@ -163,7 +163,21 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         nby_ok[d] = oky;
     }
 
-    // theta nodes (R2): t + k NTH for the first NTH threads; phi nodes (R3): t, t + NT, t + 2 NT
+    // theta nodes (R2): slot n = t + k NTH of the first NTH threads; phi nodes
+    // (R3): t, t + NT, t + 2 NT.  Slot n maps to the first TX columns of each
+    // row of the theta region, one row per warp, then to the remaining
+    // R2X - TX columns of every row: a warp's loads from the rings then stay
+    // in one row, 32 consecutive words, instead of straddling two rows of the
+    // wider rings (a two-way bank conflict).  Storage stays row-major.
+    auto r2_node = [](int n, int& hx, int& hy) {
+        constexpr int MAIN = TX * Tile<TYV>::R2Y;
+        if (n < MAIN) {
+            hy = n / TX; hx = n % TX;
+        } else {
+            const int e = n - MAIN;
+            hy = e / (R2X - TX); hx = TX + e % (R2X - TX);
+        }
+    };
     int r2_off[KTH];
     bool r2_ok[KTH];
 #pragma unroll
@@ -178,7 +192,8 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         for (int k = 0; k < KTH; ++k) {
             int n = t + k * NTH;
             if (t < NTH && n < R2N) {
-                int hx = n % R2X, hy = n / R2X;
+                int hx, hy;
+                r2_node(n, hx, hy);
                 bool ok = true;
                 int gx = wrap_coord(X0 + hx - 2, nx, p.pbx, ok);
                 int gy = wrap_coord(Y0 + hy - 2, ny, p.pby, ok);
@@ -277,7 +292,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         for (int k = 0; k < KTH; ++k) {
             const int n = t + k * NTH;
             if (t >= NTH || n >= R2N) continue;
-            const int hx = n % R2X, hy = n / R2X;
+            int hx, hy;
+            r2_node(n, hx, hy);
+            const int m = hy * R2X + hx;
             const R* c = f + (hy + 1) * R3X + (hx + 1);
             const R fc = c[0];
             R sr[3], dr_[3];
@@ -287,9 +304,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 sr[r] = W1 * ((a - fc) + (e - fc)) + W0 * (b - fc);
                 dr_[r] = e - a;
             }
-            sx[n] = W1 * (sr[0] + sr[2]) + W0 * sr[1];  // S_x S_y phi - phi_c
-            gg[n] = W1 * (W1 * (dr_[0] + dr_[2]) + W0 * dr_[1]);
-            gg[R2N + n] = W1 * (sr[2] - sr[0]);
+            sx[m] = W1 * (sr[0] + sr[2]) + W0 * sr[1];  // S_x S_y phi - phi_c
+            gg[m] = W1 * (W1 * (dr_[0] + dr_[2]) + W0 * dr_[1]);
+            gg[R2N + m] = W1 * (sr[2] - sr[0]);
         }
     };
     // theta = phi(1-phi) n on the theta region and g~ = n |g| on the collision
@@ -312,7 +329,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         for (int k = 0; k < KTH; ++k) {
             const int n = t + k * NTH;
             if (t >= NTH || n >= R2N) continue;
-            const int hx = n % R2X, hy = n / R2X;
+            int hx, hy;
+            r2_node(n, hx, hy);
+            const int m = hy * R2X + hx;
             bool fluid = zok && r2_ok[k];
             if (fluid && obs) {
                 const int s = p.isf[wz * plane + r2_off[k]];
@@ -320,10 +339,10 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             }
             R th0 = 0, th1 = 0, th2 = 0, gv0 = 0, gv1 = 0, gv2 = 0;
             if (fluid) {
-                const R gx = R(3) * (W1 * (g0[n] + g2[n]) + W0 * g1[n]);
-                const R gy = R(3) * (W1 * (g0[R2N + n] + g2[R2N + n]) + W0 * g1[R2N + n]);
+                const R gx = R(3) * (W1 * (g0[m] + g2[m]) + W0 * g1[m]);
+                const R gy = R(3) * (W1 * (g0[R2N + m] + g2[R2N + m]) + W0 * g1[R2N + m]);
                 const int c3 = (hy + 1) * R3X + (hx + 1);
-                const R gz = R(3) * W1 * ((s2[n] - s0[n]) + (f2[c3] - f0[c3]));
+                const R gz = R(3) * W1 * ((s2[m] - s0[m]) + (f2[c3] - f0[c3]));
                 const R mg = sqrt_a<R>(gx * gx + gy * gy + gz * gz);
                 const R rden = rcp<R>(mg + R(1.0e-9));
                 const R nxv = gx * rden, nyv = gy * rden, nzv = gz * rden;
@@ -332,9 +351,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 th0 = pp * nxv; th1 = pp * nyv; th2 = pp * nzv;
                 gv0 = nxv * mg; gv1 = nyv * mg; gv2 = nzv * mg;
             }
-            th[0 * R2N + n] = th0;
-            th[1 * R2N + n] = th1;
-            th[2 * R2N + n] = th2;
+            th[0 * R2N + m] = th0;
+            th[1 * R2N + m] = th1;
+            th[2 * R2N + m] = th2;
             if (hx >= 1 && hx <= R2X - 2 && hy >= 1 && hy <= R2Y - 2) {
                 const int n1 = (hy - 1) * R1X + (hx - 1);
                 gt[0 * R1N + n1] = gv0;
