@@ -17,7 +17,6 @@
 //           2-node ring) and of theta (tile + 1-node ring)
 //   theta = phi(1-phi) n on the tile + 2-node ring and g~ = n|grad phi| on
 //           the tile + 1-node ring
-//   the moments (and u_old) of plane q staged by cp.async
 //   post-collision populations of plane q on the tile + 1-node ring.
 // Each output node then pulls f*_l(x - c_l) from shared memory: the nine
 // (cx,cy) populations of each cz slice of plane q go to output plane q+cz,

@@ -6,10 +6,9 @@
 //            shared memory).  The two sets of work are independent, so one
 //            barrier covers both, and the halo-ring collisions are placed on
 //            the warps with the least theta work.
-//   phase 2  asynchronous copies (cp.async) of the next plane's moments /
-//            u_old into a shared staging area and of phi(q+4) into its ring
+//   phase 2  an asynchronous copy (cp.async) of phi(q+4) into its ring
 //            slot; then every output node pulls the populations of plane q
-//            and plane q-1 is written.  The copies complete behind this phase.
+//            and plane q-1 is written.  The copy completes behind this phase.
 #pragma once
 #include "lbf_stream.cuh"
 
@@ -53,14 +52,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Smagorinsky constant of the reference: the single-precision product 0.053 * 18.0
 constexpr double SMAG_C = (double)(0.053f * 18.0f);
 
-// fields staged per collision node: 10 moments (+3 u_old with a density ratio)
-constexpr int NSTAGE = 13;
-
-// FP32 storage is prefetched with cp.async into a staging area on tiles of 16
-// rows; 16-bit and FP64 storage, and tiles of 8 rows, read at the point of use
-// (FP64 leaves no shared memory for a staging area; without it an 8-row tile
-// needs 99 KB and two CTAs share an SM)
-template <typename S, int TYV> constexpr bool staged() { return sizeof(S) == 4 && TYV > 8; }
+// The moments (and u_old) of a collision node are read from global memory at
+// the point of use, in every storage format and tile.  A cp.async prefetch of
+// them into a shared staging area, one plane ahead, lost more than it hid: its
+// shared-memory writes were bank-conflicted (13.6 M of the 19.8 M conflicts of a
+// 256^3 FP32 launch) and the extra 52 B/node of shared traffic competed with the
+// population exchange; without it the FP32 Laplace step ran 14.1 against 12.0
+// GLUPS.
 
 // ring slots of the separable phase-field stencils (see step_body)
 constexpr int SXY_SLOTS = 5, GXY_SLOTS = 3, TH_SLOTS = 2, GT_SLOTS = 3, H_SLOTS = 3;
@@ -76,7 +74,6 @@ template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t st
     if (TC)
         b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(SXY_SLOTS) * R2N + size_t(GXY_SLOTS) * 2 * R2N +
                           size_t(TH_SLOTS) * 3 * R2N + size_t(GT_SLOTS) * 3 * R1N + size_t(H_SLOTS) * 3 * R1N);
-    if (staged<S, TYV>()) b += sizeof(S) * size_t(NSTAGE) * R1N;
     return b;
 }
 
@@ -94,7 +91,6 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     using CD = Codec<S>;
     using SP = typename PhiStore<S>::type;
     using CP = Codec<SP>;
-    constexpr bool STG = staged<S, TYV>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // post-collision populations of plane q, by (cx, cy) group g = 3 (cy+1) + (cx+1):
     // the output nodes that read one group of a node read all three cz of it
@@ -107,7 +103,6 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     R* ths = gxys + (TC ? GXY_SLOTS * 2 * R2N : 0);    // [TH_SLOTS][3][R2N]   (TC) theta
     R* gts = ths + (TC ? TH_SLOTS * 3 * R2N : 0);      // [GT_SLOTS][3][R1N]   (TC) g~
     R* hs = gts + (TC ? GT_SLOTS * 3 * R1N : 0);       // [H_SLOTS][3][R1N]    (TC) theta partials
-    S* stg = reinterpret_cast<S*>(hs + (TC ? H_SLOTS * 3 * R1N : 0));  // [NSTAGE][R1N] (STG)
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
@@ -244,28 +239,6 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             }
         }
     };
-    // moments (+ u_old) of plane q for the collision nodes of this thread
-    auto stage_plane = [&](int q) {
-        if constexpr (STG) {
-            bool zok = true;
-            const int wz = zwrap(q, zok);
-            if (!zok) return;
-            const int zo = wz * plane;
-#pragma unroll 1
-            for (int k = 0; k < 2; ++k) {
-                const int node = k ? nodeB : nodeA;
-                const bool ok = k ? okB : okA;
-                if (node < 0 || !ok) continue;
-                const int g = zo + (k ? offB : offA);
-#pragma unroll
-                for (int f = 0; f < 10; ++f) cp_async<sizeof(S)>(stg + f * R1N + node, p.min + f * N + g);
-                if (dr) {
-#pragma unroll
-                    for (int f = 0; f < 3; ++f) cp_async<sizeof(S)>(stg + (10 + f) * R1N + node, p.uin + f * N + g);
-                }
-            }
-        }
-    };
     // Separable phase-field stencils.  The isotropic gradient, Laplacian and
     // divergence of the reference (lb_cuda_auxfields_module.f90:72-135,
     // 1136-1157) use the D3Q27 weights w = W(cx) W(cy) W(cz), W(0) = 2/3,
@@ -394,7 +367,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 #pragma unroll
     for (int i = 0; i < 10; ++i) am[i] = a0[i] = ap[i] = R(0);
 
-    // ---- prologue: phi(z0-3..z0+2), theta(z0-2..z0), staged moments of plane z0-1 ----
+    // ---- prologue: phi(z0-3..z0+2), theta(z0-2..z0) ----
     if constexpr (TC) {
         // partials of phi(z0-3..z0+1), theta(z0-2..z0), theta partials (z0-2, z0-1)
         // (theta reads only this thread's own partials; the partial slots are
@@ -415,7 +388,6 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         theta_plane(z0);               // into the slot of theta(z0-2)
         load_phi_plane(z0 + 2, true);  // into the slot of phi(z0-3), no longer read
     }
-    stage_plane(z0 - 1);
     cp_async_wait_all();
     __syncthreads();
 
@@ -449,28 +421,21 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             R sP = 0, spxx = 0, spyy = 0, spzz = 0, spxy = 0, spxz = 0, spyz = 0, som = 0;
             if (live) {
                 R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;
-                if constexpr (STG) {
-                    P = (R)stg[0 * R1N + node]; u = (R)stg[1 * R1N + node];
-                    v = (R)stg[2 * R1N + node]; w = (R)stg[3 * R1N + node];
-                    pxx = (R)stg[4 * R1N + node]; pyy = (R)stg[5 * R1N + node]; pzz = (R)stg[6 * R1N + node];
-                    pxy = (R)stg[7 * R1N + node]; pxz = (R)stg[8 * R1N + node]; pyz = (R)stg[9 * R1N + node];
-                } else {
-                    if constexpr (CD::scaled) P = (R)__ldg(p.pres_in + gi);
-                    else P = CD::ld(p.min + 0 * N, gi, p.inv_scale[0]);
-                    u = CD::ld(p.min + 1 * N, gi, p.inv_scale[1]);
-                    v = CD::ld(p.min + 2 * N, gi, p.inv_scale[2]);
-                    w = CD::ld(p.min + 3 * N, gi, p.inv_scale[3]);
-                    pxx = CD::ld(p.min + 4 * N, gi, p.inv_scale[4]);
-                    pyy = CD::ld(p.min + 5 * N, gi, p.inv_scale[5]);
-                    pzz = CD::ld(p.min + 6 * N, gi, p.inv_scale[6]);
-                    pxy = CD::ld(p.min + 7 * N, gi, p.inv_scale[7]);
-                    pxz = CD::ld(p.min + 8 * N, gi, p.inv_scale[8]);
-                    pyz = CD::ld(p.min + 9 * N, gi, p.inv_scale[9]);
-                    if constexpr (CD::scaled) {
-                        // 16-bit storage keeps Pi - u u, the deviation from equilibrium
-                        pxx += u * u; pyy += v * v; pzz += w * w;
-                        pxy += u * v; pxz += u * w; pyz += v * w;
-                    }
+                if constexpr (CD::scaled) P = (R)__ldg(p.pres_in + gi);
+                else P = CD::ld(p.min + 0 * N, gi, p.inv_scale[0]);
+                u = CD::ld(p.min + 1 * N, gi, p.inv_scale[1]);
+                v = CD::ld(p.min + 2 * N, gi, p.inv_scale[2]);
+                w = CD::ld(p.min + 3 * N, gi, p.inv_scale[3]);
+                pxx = CD::ld(p.min + 4 * N, gi, p.inv_scale[4]);
+                pyy = CD::ld(p.min + 5 * N, gi, p.inv_scale[5]);
+                pzz = CD::ld(p.min + 6 * N, gi, p.inv_scale[6]);
+                pxy = CD::ld(p.min + 7 * N, gi, p.inv_scale[7]);
+                pxz = CD::ld(p.min + 8 * N, gi, p.inv_scale[8]);
+                pyz = CD::ld(p.min + 9 * N, gi, p.inv_scale[9]);
+                if constexpr (CD::scaled) {
+                    // 16-bit storage keeps Pi - u u, the deviation from equilibrium
+                    pxx += u * u; pyy += v * v; pzz += w * w;
+                    pxy += u * v; pxz += u * w; pyz += v * w;
                 }
                 R phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
                 if constexpr (TC) {
@@ -533,14 +498,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 }
                 R tfx = fxv, tfy = fyv, tfz = fzv;
                 if (dr) {
-                    R uo, vo, wo;
-                    if constexpr (STG) {
-                        uo = (R)stg[10 * R1N + node]; vo = (R)stg[11 * R1N + node]; wo = (R)stg[12 * R1N + node];
-                    } else {
-                        uo = CD::ld(p.uin + 0 * N, gi, p.inv_scale[F_UOLD + 0]);
-                        vo = CD::ld(p.uin + 1 * N, gi, p.inv_scale[F_UOLD + 1]);
-                        wo = CD::ld(p.uin + 2 * N, gi, p.inv_scale[F_UOLD + 2]);
-                    }
+                    const R uo = CD::ld(p.uin + 0 * N, gi, p.inv_scale[F_UOLD + 0]);
+                    const R vo = CD::ld(p.uin + 1 * N, gi, p.inv_scale[F_UOLD + 1]);
+                    const R wo = CD::ld(p.uin + 2 * N, gi, p.inv_scale[F_UOLD + 2]);
                     const R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
                     const R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
                     const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
@@ -739,8 +699,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         __syncthreads();
 
         // ================= phase 2 =================
-        // the staging area and the slot of phi(q-1) were last read in phase 1
-        if (q < z1) stage_plane(q + 1);
+        // the slot of phi(q-1) was last read in phase 1
         if constexpr (TC) load_phi_plane(q + 4, true);
 
         // the three cz populations of every (cx, cy) group from node x - c
