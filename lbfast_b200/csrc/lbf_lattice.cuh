@@ -78,15 +78,21 @@ template <typename R> __device__ __forceinline__ R fmaf_t(R a, R b, R c) { retur
 // storage codecs: fields live in HBM as S; arithmetic is in R.  Scaled 16-bit
 // storage keeps value*scale (scale per field, chosen on the host).
 // ---------------------------------------------------------------------------
+// ld = raw + dec: raw issues the load of a stored value, dec turns it into
+// the arithmetic type, so a load can be issued well before its value is used
 template <typename S> struct Codec;
 template <> struct Codec<float> {
     static constexpr bool scaled = false;
     template <typename R> __device__ static R ld(const float* p, long long i, R) { return (R)__ldg(p + i); }
+    __device__ static float raw(const float* p, long long i) { return __ldg(p + i); }
+    template <typename R> __device__ static R dec(float s, R) { return (R)s; }
     template <typename R> __device__ static void st(float* p, long long i, R v, R) { p[i] = (float)v; }
 };
 template <> struct Codec<double> {
     static constexpr bool scaled = false;
     template <typename R> __device__ static R ld(const double* p, long long i, R) { return (R)__ldg(p + i); }
+    __device__ static double raw(const double* p, long long i) { return __ldg(p + i); }
+    template <typename R> __device__ static R dec(double s, R) { return (R)s; }
     template <typename R> __device__ static void st(double* p, long long i, R v, R) { p[i] = (double)v; }
 };
 template <> struct Codec<__half> {
@@ -94,6 +100,8 @@ template <> struct Codec<__half> {
     template <typename R> __device__ static R ld(const __half* p, long long i, R inv) {
         return (R)__half2float(__ldg(p + i)) * inv;
     }
+    __device__ static __half raw(const __half* p, long long i) { return __ldg(p + i); }
+    template <typename R> __device__ static R dec(__half s, R inv) { return (R)__half2float(s) * inv; }
     template <typename R> __device__ static void st(__half* p, long long i, R v, R sc) {
         p[i] = __float2half_rn((float)(v * sc));
     }
@@ -103,6 +111,8 @@ template <> struct Codec<__nv_bfloat16> {
     template <typename R> __device__ static R ld(const __nv_bfloat16* p, long long i, R inv) {
         return (R)__bfloat162float(__ldg(p + i)) * inv;
     }
+    __device__ static __nv_bfloat16 raw(const __nv_bfloat16* p, long long i) { return __ldg(p + i); }
+    template <typename R> __device__ static R dec(__nv_bfloat16 s, R inv) { return (R)__bfloat162float(s) * inv; }
     template <typename R> __device__ static void st(__nv_bfloat16* p, long long i, R v, R sc) {
         p[i] = __float2bfloat16_rn((float)(v * sc));
     }

@@ -52,9 +52,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Smagorinsky constant of the reference: the single-precision product 0.053 * 18.0
 constexpr double SMAG_C = (double)(0.053f * 18.0f);
 
-// The moments (and u_old) of a collision node are read from global memory at
-// the point of use, in every storage format and tile.  A cp.async prefetch of
-// them into a shared staging area, one plane ahead, lost more than it hid: its
+// The moments (and u_old) of a collision node go from global memory straight
+// into registers: the tile-interior node's one plane ahead (NodeRaw, below),
+// the ring nodes' at the point of use.  A cp.async prefetch of them into a
+// shared staging area, one plane ahead, lost more than it hid: its
 // shared-memory writes were bank-conflicted (13.6 M of the 19.8 M conflicts of a
 // 256^3 FP32 launch) and the extra 52 B/node of shared traffic competed with the
 // population exchange; without it the FP32 Laplace step ran 14.1 against 12.0
@@ -361,6 +362,34 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         }
     };
 
+    // stored moments, u_old and isfluid of one collision node, not yet decoded.
+    // The tile-interior node's are loaded one plane ahead, at the start of the
+    // pull phase of the plane before, so their latency passes behind that
+    // phase and its barrier; the ring nodes load theirs at the point of use.
+    struct NodeRaw {
+        S m[10];
+        float P;  // 32-bit P of the scaled formats (m[0] unused there)
+        S uo[3];
+        int8_t isf;
+    };
+    auto fetch = [&](int gi, NodeRaw& r) {
+        if constexpr (CD::scaled) r.P = __ldg(p.pres_in + gi);
+        else r.m[0] = CD::raw(p.min, gi);
+#pragma unroll
+        for (int f = 1; f < 10; ++f) r.m[f] = CD::raw(p.min + f * N, gi);
+        if (dr) {
+#pragma unroll
+            for (int f = 0; f < 3; ++f) r.uo[f] = CD::raw(p.uin + f * N, gi);
+        }
+        if (obs) r.isf = p.isf[gi];
+    };
+    NodeRaw nxt;
+    auto prefetch_a = [&](int q) {
+        bool zk = true;
+        const int wz = zwrap(q, zk);
+        if (zk && okA) fetch(wz * plane + offA, nxt);
+    };
+
     // accumulators of the raw moments {sum g, sum g c, sum g c c} for output planes
     // q-1 (am), q (a0), q+1 (ap)
     R am[10], a0[10], ap[10];
@@ -388,6 +417,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         theta_plane(z0);               // into the slot of theta(z0-2)
         load_phi_plane(z0 + 2, true);  // into the slot of phi(z0-3), no longer read
     }
+    prefetch_a(z0 - 1);
     cp_async_wait_all();
     __syncthreads();
 
@@ -413,25 +443,28 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             if (node < 0) continue;
             const bool inb = zok && (k ? okB : okA);
             const int gi = zoff + (k ? offB : offA);
+            NodeRaw cur;
+            if (k == 0) cur = nxt;
+            else if (inb) fetch(gi, cur);
             int isf = 1;
-            if (inb && obs) isf = p.isf[gi];
+            if (inb && obs) isf = cur.isf;
             const bool live = inb && (isf != 0);
             const bool interior = (k == 0) && out_ok && q_inner;
             R fpop[27];
             R sP = 0, spxx = 0, spyy = 0, spzz = 0, spxy = 0, spxz = 0, spyz = 0, som = 0;
             if (live) {
                 R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;
-                if constexpr (CD::scaled) P = (R)__ldg(p.pres_in + gi);
-                else P = CD::ld(p.min + 0 * N, gi, p.inv_scale[0]);
-                u = CD::ld(p.min + 1 * N, gi, p.inv_scale[1]);
-                v = CD::ld(p.min + 2 * N, gi, p.inv_scale[2]);
-                w = CD::ld(p.min + 3 * N, gi, p.inv_scale[3]);
-                pxx = CD::ld(p.min + 4 * N, gi, p.inv_scale[4]);
-                pyy = CD::ld(p.min + 5 * N, gi, p.inv_scale[5]);
-                pzz = CD::ld(p.min + 6 * N, gi, p.inv_scale[6]);
-                pxy = CD::ld(p.min + 7 * N, gi, p.inv_scale[7]);
-                pxz = CD::ld(p.min + 8 * N, gi, p.inv_scale[8]);
-                pyz = CD::ld(p.min + 9 * N, gi, p.inv_scale[9]);
+                if constexpr (CD::scaled) P = (R)cur.P;
+                else P = CD::dec(cur.m[0], p.inv_scale[0]);
+                u = CD::dec(cur.m[1], p.inv_scale[1]);
+                v = CD::dec(cur.m[2], p.inv_scale[2]);
+                w = CD::dec(cur.m[3], p.inv_scale[3]);
+                pxx = CD::dec(cur.m[4], p.inv_scale[4]);
+                pyy = CD::dec(cur.m[5], p.inv_scale[5]);
+                pzz = CD::dec(cur.m[6], p.inv_scale[6]);
+                pxy = CD::dec(cur.m[7], p.inv_scale[7]);
+                pxz = CD::dec(cur.m[8], p.inv_scale[8]);
+                pyz = CD::dec(cur.m[9], p.inv_scale[9]);
                 if constexpr (CD::scaled) {
                     // 16-bit storage keeps Pi - u u, the deviation from equilibrium
                     pxx += u * u; pyy += v * v; pzz += w * w;
@@ -498,9 +531,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 }
                 R tfx = fxv, tfy = fyv, tfz = fzv;
                 if (dr) {
-                    const R uo = CD::ld(p.uin + 0 * N, gi, p.inv_scale[F_UOLD + 0]);
-                    const R vo = CD::ld(p.uin + 1 * N, gi, p.inv_scale[F_UOLD + 1]);
-                    const R wo = CD::ld(p.uin + 2 * N, gi, p.inv_scale[F_UOLD + 2]);
+                    const R uo = CD::dec(cur.uo[0], p.inv_scale[F_UOLD + 0]);
+                    const R vo = CD::dec(cur.uo[1], p.inv_scale[F_UOLD + 1]);
+                    const R wo = CD::dec(cur.uo[2], p.inv_scale[F_UOLD + 2]);
                     const R qxx = pxx - uo * uo, qyy = pyy - vo * vo, qzz = pzz - wo * wo;
                     const R qxy = pxy - uo * vo, qxz = pxz - uo * wo, qyz = pyz - vo * wo;
                     const R visc = (p.rho_r * p.visc1 * phi + (R(1) - phi) * p.visc2 * p.rho_b) * inv;
@@ -700,6 +733,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 
         // ================= phase 2 =================
         // the slot of phi(q-1) was last read in phase 1
+        prefetch_a(q + 1);
         if constexpr (TC) load_phi_plane(q + 4, true);
 
         // the three cz populations of every (cx, cy) group from node x - c
