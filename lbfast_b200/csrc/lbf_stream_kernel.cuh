@@ -341,7 +341,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     auto theta_partials = [&](int q) {
         const R* th = ths + th_slot(q) * (3 * R2N);
         R* h = hs + h_slot(q) * (3 * R1N);
-#pragma unroll 1
+#pragma unroll
         for (int k = 0; k < 2; ++k) {
             const int node = k ? nodeB : nodeA;
             if (node < 0) continue;
