@@ -180,9 +180,9 @@ int lbf_reduce(lbf_handle* h, double out[5]);
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory while they run: a Fortran integrator whose device
  * arrays belong to OpenACC data regions and reach the library only as device
- * pointers, a time loop captured into a CUDA graph (cudaMalloc cannot be
- * captured and synchronises the device), a solver held to a fixed device
- * memory budget.  Computes the same FP64 sums as lbf_reduce -- phi, P, u, v,
+ * pointers, a host application that hands out all device memory from its
+ * own pool, a solver held to a fixed device memory budget (an allocation
+ * inside a call could fail or push it over).  Computes the same FP64 sums as lbf_reduce -- phi, P, u, v,
  * w over nodes with isfluid = 1 or -1 -- over caller-owned device arrays:
  * mom10 (float, 10 x lx*ly*lz, only the first four fields are read), phi
  * (float, may be NULL), isfluid (int8, may be NULL = all fluid).  out is a

@@ -4,9 +4,10 @@
 // Some callers cannot let a library allocate device memory while they run:
 // a Fortran integrator whose device arrays live inside OpenACC data regions
 // owns every device buffer and hands the library only device pointers; a
-// time loop captured into a CUDA graph cannot contain cudaMalloc (it is not
-// a capturable operation, and it synchronises the device); a solver running
-// inside a fixed device-memory budget cannot have a call grow its footprint.
+// host application that hands out all device memory from its own pool does
+// not want a second allocator beside it; a solver running inside a fixed
+// device-memory budget cannot have a call grow its footprint (the allocation
+// could fail mid-run or push it over).
 // lbf_reduce_noalloc serves them: the caller passes the fields and receives
 // the five sums, and the only scratch the computation needs -- one partial
 // sum per z plane -- lives in a file-scope __device__ array that exists

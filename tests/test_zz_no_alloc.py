@@ -1,7 +1,7 @@
 """lbf_reduce_noalloc: the reduction for callers that cannot let the library
 allocate device memory (a Fortran integrator whose device arrays belong to
-OpenACC data regions, a time loop captured into a CUDA graph, a solver held
-to a fixed device-memory budget).  Its fields are caller-owned device arrays
+OpenACC data regions, an application that hands out all device memory from
+its own pool, a solver held to a fixed device-memory budget).  Its fields are caller-owned device arrays
 and its scratch is a static device array, so this test hands it device
 tensors holding the state of a solver and checks the sums against the
 library's allocating entry point, lbf_reduce, on the same state -- twice in a
