@@ -190,10 +190,17 @@ int lbf_reduce(lbf_handle* h, double out[5]);
  * file-scope __device__ array of LBF_NOALLOC_MAX_PLANES + 1 rows of five
  * doubles (328 KB held on every GPU that loads the library until process
  * exit); boxes with lz > LBF_NOALLOC_MAX_PLANES are rejected with LBF_E_ARG.
- * The first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race.  Runs on the legacy
- * default stream and returns after the totals reached `out`. */
+ * mom10, phi and isfluid must be device (or managed) memory of the current
+ * device: anything else -- a host address passed without `host_data
+ * use_device` -- is rejected with LBF_E_ARG before any launch.  Every call
+ * looks up the array's device address with the current device; the first
+ * call on a device also loads the kernels there, so make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  Runs on the legacy default stream, which does not wait for
+ * non-blocking streams or OpenACC async queues: the caller synchronises the
+ * stream or queue that produced the fields first (`!$acc wait`).  Returns
+ * after the totals reached `out`; LBF_E_NUMERIC (sums written) when a sum is
+ * not finite, as lbf_reduce does. */
 #define LBF_NOALLOC_MAX_PLANES 8192
 int lbf_reduce_noalloc(const float* mom10, const float* phi, const int8_t* isfluid, int lx, int ly, int lz,
                        double out[5]);

@@ -18,6 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "liblbfast_b200.so")
 
 LBF_OK = 0
+LBF_E_ARG, LBF_E_CUDA, LBF_E_NOMEM, LBF_E_STATE, LBF_E_UNSUPPORTED, LBF_E_IO, LBF_E_NUMERIC = -1, -2, -3, -4, -5, -6, -7
 STORE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
 LBF_F32, LBF_F64 = 0, 1
 

@@ -18,8 +18,15 @@
 // planes are rejected.  Every slot a call reads is written earlier in the same
 // call, so nothing needs clearing between calls; calls that overlap on the
 // GPU (other streams or host threads) share the array and race.
+//
+// The field pointers come straight from the caller, so before anything is
+// launched each one is checked to be device (or managed) memory of the
+// current device: a host address passed by mistake -- a Fortran call without
+// `host_data use_device` -- is rejected with LBF_E_ARG instead of being read
+// from the GPU.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 
 #include "../../include/lbfast_gpu.h"
@@ -32,11 +39,6 @@ constexpr int RED_THREADS = 256;
 
 static __device__ __align__(256) double g_plane_sums[(LBF_NOALLOC_MAX_PLANES + 1) * NRED];
 
-// device address of g_plane_sums, per device (host code may not name the
-// symbol as a device address)
-constexpr int MAX_DEVICES = 64;
-double* g_scratch_addr[MAX_DEVICES] = {nullptr};
-
 // failures are reported through lbf_last_error, like every other entry point
 int fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
     char buf[384];
@@ -46,6 +48,32 @@ int fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
         std::snprintf(buf, sizeof(buf), "lbf_reduce_noalloc: %s", msg);
     lbf::record_error(buf);
     return code;
+}
+
+// LBF_OK when p is device or managed memory that the current device `dev` can
+// read as a plain device pointer
+int check_device_pointer(const void* p, int dev, const char* name) {
+    cudaPointerAttributes a{};
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // the failed query leaves a (non-sticky) error behind: clear it
+        char msg[160];
+        std::snprintf(msg, sizeof(msg), "%s is not a pointer the CUDA runtime knows", name);
+        return fail(LBF_E_ARG, msg, e);
+    }
+    const bool dev_mem = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (!dev_mem || (a.type == cudaMemoryTypeDevice && a.device != dev)) {
+        char msg[200];
+        std::snprintf(msg, sizeof(msg),
+                      "%s must be device memory of the current device %d (got %s); from Fortran pass it "
+                      "inside `!$acc host_data use_device(...)`",
+                      name, dev,
+                      a.type == cudaMemoryTypeDevice ? "another device's memory"
+                      : a.type == cudaMemoryTypeHost ? "pinned host memory"
+                                                     : "host memory");
+        return fail(LBF_E_ARG, msg);
+    }
+    return LBF_OK;
 }
 
 __device__ __forceinline__ void block_sum(double (&acc)[NRED], double (*red)[RED_THREADS]) {
@@ -113,17 +141,19 @@ extern "C" int lbf_reduce_noalloc(const float* mom10, const float* phi, const in
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(LBF_E_CUDA, "cudaGetDevice failed", e);
-    if (dev < 0 || dev >= MAX_DEVICES) return fail(LBF_E_UNSUPPORTED, "device index beyond the supported range");
-    // first call on this device: resolve the device address of the scratch array
-    // (with this device current); this is a host-side query, so make it before
-    // any stream capture that contains this entry point
-    if (!g_scratch_addr[dev]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_plane_sums);
-        if (e != cudaSuccess || !ptr) return fail(LBF_E_CUDA, "cudaGetSymbolAddress of the scratch array failed", e);
-        g_scratch_addr[dev] = static_cast<double*>(ptr);
-    }
-    double* sums = g_scratch_addr[dev];
+    int rc = check_device_pointer(mom10, dev, "mom10");
+    if (rc == LBF_OK && phi) rc = check_device_pointer(phi, dev, "phi");
+    if (rc == LBF_OK && isfluid) rc = check_device_pointer(isfluid, dev, "isfluid");
+    if (rc != LBF_OK) return rc;
+    // device address of the scratch array on the current device, looked up on
+    // every call (a host-side query: host code cannot use the symbol itself as
+    // a device address, and a looked-up address would go stale after a
+    // cudaDeviceReset).  The first call on a device also loads this file's
+    // kernels there, so make it before any stream capture.
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_plane_sums);
+    if (e != cudaSuccess || !ptr) return fail(LBF_E_CUDA, "cudaGetSymbolAddress of the scratch array failed", e);
+    double* sums = static_cast<double*>(ptr);
     const long long plane = (long long)lx * ly;
     const long long n = plane * lz;
     plane_sums_kernel<<<lz, RED_THREADS>>>(mom10, phi, isfluid, plane, n, sums);
@@ -135,5 +165,13 @@ extern "C" int lbf_reduce_noalloc(const float* mom10, const float* phi, const in
     e = cudaMemcpy(out, sums + (long long)LBF_NOALLOC_MAX_PLANES * NRED, NRED * sizeof(double),
                    cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(LBF_E_CUDA, "copy of the totals failed", e);
+    // a diverged state is reported the way lbf_reduce reports it
+    static const char* const names[NRED] = {"phi", "P", "u", "v", "w"};
+    for (int k = 0; k < NRED; ++k)
+        if (!std::isfinite(out[k])) {
+            char msg[128];
+            std::snprintf(msg, sizeof(msg), "the sum of %s over the fluid is not finite", names[k]);
+            return fail(LBF_E_NUMERIC, msg);
+        }
     return LBF_OK;
 }

@@ -3,8 +3,8 @@
 Parses the `#if LATTICE == 27 / 19 / 15` blocks of vars_module.f90 (lines
 319-338, 666-684 and 685-703 of the LBFAST sources): the link vectors ex, ey,
 ez, the opposite links opp and the weights p(0:nlinks) built from the
-parameters p0..p3.  Run here, where the reference sources are mounted:
-    python tests/golden/make_lattice_golden.py /root/reference/vars_module.f90
+parameters p0..p3.  Run with the path of the LBFAST sources' vars_module.f90:
+    python tests/golden/make_lattice_golden.py <LBFAST sources>/vars_module.f90
 """
 import json
 import re

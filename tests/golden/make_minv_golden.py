@@ -3,8 +3,8 @@
 Parses the Fortran array constructor `Minv_mrt(0:nlinks,0:nlinks) = reshape([...])`
 in vars_module.f90 (lines 360-521 of the LBFAST sources) and stores it as
 minv[r, l] = Minv_mrt(r, l): r the Hermite basis row, l the population.
-Run here, where the reference sources are mounted:
-    python tests/golden/make_minv_golden.py /root/reference/vars_module.f90
+Run with the path of the LBFAST sources' vars_module.f90:
+    python tests/golden/make_minv_golden.py <LBFAST sources>/vars_module.f90
 """
 import re
 import sys

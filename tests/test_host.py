@@ -134,10 +134,12 @@ def test_namelist_reader_reads_repulsive_parameters(tmp_path):
 
 
 def test_namelist_reader_reads_reference_inputs():
-    ref = "/root/reference"
-    files = sorted(f for f in os.listdir(ref) if f.endswith(".inp")) if os.path.isdir(ref) else []
+    """Every *.inp file of the LBFAST sources, when their directory is given
+    in LBFAST_REFERENCE_DIR."""
+    ref = os.environ.get("LBFAST_REFERENCE_DIR", "")
+    files = sorted(f for f in os.listdir(ref) if f.endswith(".inp")) if ref and os.path.isdir(ref) else []
     if not files:
-        pytest.skip("reference inputs not mounted")
+        pytest.skip("LBFAST_REFERENCE_DIR does not name a directory of LBFAST .inp files")
     for f in files:
         rc, p, r = read_nml(os.path.join(ref, f))
         assert rc == 0, f

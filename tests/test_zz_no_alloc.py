@@ -65,6 +65,67 @@ def test_noalloc_reduce_matches_allocating_reduce_twice():
     s.close()
 
 
+def test_noalloc_reduce_null_phi_null_isfluid_and_many_planes():
+    """phi = NULL and isfluid = NULL (every node fluid) on 4 x 4 x 300 random
+    fields -- more z planes than the total kernel's 256 threads, so its
+    strided loop runs -- against numpy FP64 sums, twice in a row."""
+    import torch
+    lib = capi.load()
+    _bind(lib)
+    rng = np.random.default_rng(11)
+    shape = (300, 4, 4)
+    for call in range(2):
+        m = rng.standard_normal((10,) + shape).astype(np.float32)
+        m_dev = torch.from_numpy(m).cuda()
+        torch.cuda.synchronize()
+        rc, out = _noalloc(lib, m_dev, None, None, shape)
+        assert rc == capi.LBF_OK, capi.last_error()
+        ref = np.array([0.0] + [m[f].astype(np.float64).sum() for f in range(4)])
+        scale = np.array([1.0] + [np.abs(m[f]).astype(np.float64).sum() for f in range(4)])
+        assert out[0] == 0.0
+        assert np.all(np.abs(out - ref) <= 1e-12 * scale), (call, out, ref)
+    # phi given, isfluid NULL
+    phi = rng.random(shape, dtype=np.float32)
+    rc, out = _noalloc(lib, m_dev, torch.from_numpy(phi).cuda(), None, shape)
+    assert rc == capi.LBF_OK, capi.last_error()
+    assert abs(out[0] - phi.astype(np.float64).sum()) <= 1e-12 * phi.sum()
+
+
+def test_noalloc_reduce_rejects_host_pointers_before_launch():
+    """A host address (a Fortran call made outside host_data use_device) is
+    refused with LBF_E_ARG by the pointer check; nothing is launched."""
+    import torch
+    lib = capi.load()
+    _bind(lib)
+    host = np.zeros((10, 2, 2, 2), dtype=np.float32)
+    out = np.zeros(5, dtype=np.float64)
+    rc = lib.lbf_reduce_noalloc(C.c_void_p(host.ctypes.data), None, None, 2, 2, 2,
+                                out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == capi.LBF_E_ARG
+    assert "mom10" in capi.last_error()
+    dev = torch.zeros((10, 2, 2, 2), dtype=torch.float32, device="cuda")
+    rc = lib.lbf_reduce_noalloc(C.c_void_p(dev.data_ptr()), C.c_void_p(host.ctypes.data), None, 2, 2, 2,
+                                out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == capi.LBF_E_ARG
+    assert "phi" in capi.last_error()
+    # the context is intact: a valid call still works
+    rc = lib.lbf_reduce_noalloc(C.c_void_p(dev.data_ptr()), None, None, 2, 2, 2,
+                                out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == capi.LBF_OK, capi.last_error()
+
+
+def test_noalloc_reduce_reports_non_finite_sums():
+    """A NaN in the fields returns LBF_E_NUMERIC (sums still written), as lbf_reduce does."""
+    import torch
+    lib = capi.load()
+    _bind(lib)
+    m = np.zeros((10, 3, 3, 3), dtype=np.float32)
+    m[2, 1, 1, 1] = np.nan
+    rc, out = _noalloc(lib, torch.from_numpy(m).cuda(), None, None, (3, 3, 3))
+    assert rc == capi.LBF_E_NUMERIC
+    assert np.isnan(out[3]) and "u" in capi.last_error()
+
+
 def test_noalloc_reduce_rejects_boxes_beyond_its_scratch():
     import torch
     lib = capi.load()
