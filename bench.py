@@ -23,6 +23,16 @@ Arms:
                    Fortran/OpenACC and cannot be built here), FP32, all host
                    threads, on a bounded number of steps of the same box.
 
+Beside the headline the line carries "extra": device-resident MLUPS and
+roofline of the other configurations the metric names -- FP16 storage on the
+same box, the 512 x 256 x 256 channel with obstacles (FP32) and the 768^3
+box of 200 seeded droplets (FP32 and FP16 storage) -- each timed the same
+way on fewer steps.  "cpu_baseline" holds the oracle on the headline box
+and, as "taylor_green", the 64^3 D3Q19 Taylor-Green case at its full 1000
+steps.  Clocks are sampled by nvidia-smi over a window of steady stepping
+that contains the timed steps (a second of steps before them, a fraction
+after).
+
 Multi-GPU (torchrun): every rank advances its own replica of the box (the
 single-GPU path has no exchange step); "value" sums the ranks' lattice
 updates over the slowest rank's time.
@@ -54,14 +64,26 @@ NCU_TRAFFIC = {("f32", 256): 1854044160}
 CHANNEL = (512, 256, 256)  # the two-component channel with obstacles (lx, ly, lz)
 
 
-def channel_geometry(lx=CHANNEL[0], ly=CHANNEL[1], lz=CHANNEL[2]):
+def _helpers(oracle_helpers: bool):
+    """Set-up helpers (isfluid marking, solid phi seeding, the droplet initial
+    condition): the library's, or the oracle's numpy restatements of the same
+    reference routines -- the reference arm uses those, so it never loads the
+    product library."""
+    if oracle_helpers:
+        from oracle import oracle as O
+        return O.mark_isfluid, O.seed_solid_phi, O.ic_droplet
+    import lbfast_b200 as lbf
+    return lbf.mark_isfluid, lbf.seed_solid_phi, lbf.ic_droplet
+
+
+def channel_geometry(lx=CHANNEL[0], ly=CHANNEL[1], lz=CHANNEL[2], oracle_helpers=False):
     """isfluid and phi of the channel: walls at y = 0 and ly-1 (pbc 1, 0, 1),
     64 seeded solid spheres of radius U[6, 14] kept clear of the periodic faces
     (seed 12345), phi from 32 seeded blobs of radius U[8, 24] with a width-4
     tanh profile (seed 67890), solid-node phi seeded from fluid neighbours."""
     import numpy as np
 
-    import lbfast_b200 as lbf
+    mark_isfluid, seed_solid_phi, _ = _helpers(oracle_helpers)
     rng = np.random.default_rng(12345)
     solid = np.zeros((lz, ly, lx), dtype=bool)
     for _ in range(64):
@@ -73,7 +95,10 @@ def channel_geometry(lx=CHANNEL[0], ly=CHANNEL[1], lz=CHANNEL[2]):
         x0, x1 = int(c[0] - r) - 1, int(c[0] + r) + 2
         z, y, x = np.ogrid[z0:z1, y0:y1, x0:x1]
         solid[z0:z1, y0:y1, x0:x1] |= (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r
-    isf = lbf.mark_isfluid(np.where(solid, 0, 1).astype(np.int8), (1, 0, 1), 27, True)
+    if oracle_helpers:
+        isf = mark_isfluid(solid, (1, 0, 1), 27, True)
+    else:
+        isf = mark_isfluid(np.where(solid, 0, 1).astype(np.int8), (1, 0, 1), 27, True)
     rng = np.random.default_rng(67890)
     phi = np.zeros((lz, ly, lx))
     for _ in range(32):
@@ -90,38 +115,85 @@ def channel_geometry(lx=CHANNEL[0], ly=CHANNEL[1], lz=CHANNEL[2]):
         sub = phi[np.ix_(zi, yi, xi)]
         phi[np.ix_(zi, yi, xi)] = np.maximum(sub, blob)
     phi = np.where(isf == 0, 0.0, phi)
-    phi = lbf.seed_solid_phi(phi, isf, 27)
+    phi = seed_solid_phi(phi, isf, 27)
     return isf, phi
 
 
-def workload(storage: str = "f32", L: int = LBOX, kind: str = "laplace"):
+def droplets_field(L: int, n: int = 200, seed: int = 2024, rmin: float = 10.0, rmax: float = 30.0,
+                   width: float = 4.0, sigma: float = 0.01, rho_r: float = 5.0, rho_b: float = 0.5):
+    """Moments and phi (float32) of a periodic L^3 box holding n seeded
+    droplets (centres U[0,L)^3, radii U[rmin, rmax], the fcut_tanh profile of
+    width 4) at rest, each node's P the Laplace pressure of the droplet that
+    dominates it (init_conditions_module.f90:413-414)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    phi = np.zeros((L, L, L), np.float32)
+    press = np.zeros((L, L, L), np.float32)
+    for _ in range(n):
+        c = rng.uniform(0.0, L, 3)
+        r = rng.uniform(rmin, rmax)
+        h = int(r + 2 * width) + 1
+        idx = [np.arange(int(c[d]) - h, int(c[d]) + h + 1) for d in range(3)]
+        d2 = ((idx[2][:, None, None] - c[2]) ** 2 + (idx[1][None, :, None] - c[1]) ** 2 +
+              (idx[0][None, None, :] - c[0]) ** 2)
+        f = (0.5 * (1.0 - np.tanh((np.sqrt(d2) - r) / (0.5 * width)))).astype(np.float32)
+        ix = np.ix_(idx[2] % L, idx[1] % L, idx[0] % L)
+        sub = phi[ix]
+        take = f > sub
+        rhophi = rho_r * f + (1.0 - f) * rho_b
+        pr = (f * (2.0 * sigma) / r / (rhophi / 3.0)).astype(np.float32)
+        phi[ix] = np.where(take, f, sub)
+        press[ix] = np.where(take, pr, press[ix])
+    m = np.zeros((10, L, L, L), np.float32)
+    m[0] = press
+    return m, phi
+
+
+def workload(storage: str = "f32", L: int = LBOX, kind: str = "laplace", oracle_helpers: bool = False):
     """(Params, moments, phi, isfluid or None) of the Laplace droplet (L^3,
-    the headline) or of the channel with obstacles (512 x 256 x 256: walls,
+    the headline), of the channel with obstacles (512 x 256 x 256: walls,
     spheres and wetting at 90 degrees, body force 1e-6, the twopoiseuille.inp
-    fluid parameters)."""
+    fluid parameters), of the box of 200 seeded droplets (L^3, the bench.inp
+    fluid parameters) or of the Taylor-Green vortex (64^3 D3Q19, one
+    component)."""
     import numpy as np
 
-    import lbfast_b200 as lbf
+    from lbfast_b200.capi import Params
+    _, _, ic_droplet = _helpers(oracle_helpers)
     if kind == "channel":
         lx, ly, lz = CHANNEL
-        p = lbf.Params(lx=lx, ly=ly, lz=lz, pbc_y=0, lattice=27, highorder=1, twocomponent=1, densratio=1,
-                       obstacles=1, visc1=0.05, visc2=0.4, rho_r=0.5, rho_b=1.5, sigma=0.0, width=4.0,
-                       tau_diff=0.1, fx=1e-6, wettab_r=90.0, printphi=1, storage=storage)
-        isf, phi = channel_geometry(lx, ly, lz)
+        p = Params(lx=lx, ly=ly, lz=lz, pbc_y=0, lattice=27, highorder=1, twocomponent=1, densratio=1,
+                   obstacles=1, visc1=0.05, visc2=0.4, rho_r=0.5, rho_b=1.5, sigma=0.0, width=4.0,
+                   tau_diff=0.1, fx=1e-6, wettab_r=90.0, printphi=1, storage=storage)
+        isf, phi = channel_geometry(lx, ly, lz, oracle_helpers)
         return p, np.zeros((10, lz, ly, lx)), phi, isf
-    p = lbf.Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1,
-                   visc1=0.1, visc2=0.1, rho_r=RHO_R, rho_b=RHO_B, sigma=0.03, width=3.0, tau_diff=0.1,
+    if kind == "droplets":
+        p = Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1, visc1=0.2,
+                   visc2=0.025, rho_r=5.0, rho_b=0.5, sigma=0.01, width=4.0, tau_diff=0.12, fx=1e-6,
                    printphi=1, storage=storage)
+        m, phi = droplets_field(L)
+        return p, m, phi, None
+    if kind == "taylorgreen":
+        from oracle import oracle as O
+        p = Params(lx=64, ly=64, lz=64, lattice=19, visc1=0.01, storage=storage)
+        return p, O.ic_taylor_green(64, 64, 64, 0.05), None, None
+    p = Params(lx=L, ly=L, lz=L, lattice=27, highorder=1, twocomponent=1, densratio=1,
+               visc1=0.1, visc2=0.1, rho_r=RHO_R, rho_b=RHO_B, sigma=0.03, width=3.0, tau_diff=0.1,
+               printphi=1, storage=storage)
     R = 40.0 * L / 256
-    m, phi = lbf.ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, RHO_R, RHO_B, True)
+    m, phi = ic_droplet(L, L, L, (L / 2, L / 2, L / 2), R, 3.0, 0.03, RHO_R, RHO_B, True)
     return p, m, phi, None
 
 
 def box_of(kind, L=LBOX):
+    if kind == "taylorgreen":
+        return [64, 64, 64]
     return list(CHANNEL) if kind == "channel" else [L, L, L]
 
 
 def bytes_per_lup(storage, kind):
+    if kind == "taylorgreen":
+        return {"f32": 80, "f64": 160}.get(storage, 44)  # one component: 10 moments
     return B_LUP[storage] + (1 if kind == "channel" else 0)  # + the isfluid byte with obstacles
 
 
@@ -133,25 +205,41 @@ def config_dict(storage, L=LBOX, kind="laplace"):
         text = ("two-component channel with obstacles 512x256x256, D3Q27 HIGHORDER DENSRATIO (rho 0.5/1.5, "
                 "nu 0.05/0.4), walls at y = 0 and 255, 64 seeded spheres R U[6,14], seeded phi blobs, "
                 "wetting 90 degrees, fx 1e-6, fluids at rest")
+    elif kind == "droplets":
+        text = (f"{L}^3 periodic, 200 seeded droplets R U[10,30] (seed 2024, width 4), D3Q27 HIGHORDER "
+                f"two-component DENSRATIO (rho 5/0.5, nu 0.2/0.025, sigma 0.01, tau_diff 0.12, fx 1e-6)")
+    elif kind == "taylorgreen":
+        text = "Taylor-Green vortex 64^3 periodic, one-component D3Q19, nu 0.01, u0 0.05, 1000 steps"
     else:
         text = (f"Laplace droplet {L}^3 periodic, D3Q27 HIGHORDER two-component DENSRATIO "
                 f"(rho_r/rho_b = {RHO_R:g}/{RHO_B:g}), R={int(40 * L / 256)}, width 3, sigma 0.03")
-    return {"workload": text, "box": box, "lattice": "D3Q27", "highorder": True, "twocomponent": True,
-            "densratio": True, "obstacles": kind == "channel", "storage": storage, "bytes_per_lup": b,
+    tg = kind == "taylorgreen"
+    return {"workload": text, "box": box, "lattice": "D3Q19" if tg else "D3Q27", "highorder": not tg,
+            "twocomponent": not tg, "densratio": not tg, "obstacles": kind == "channel", "storage": storage,
+            "bytes_per_lup": b,
             "l2_policy": ("state (%.2f GB) larger than the 126 MB L2; no flush" % (n * b / 1e9)
                           if n * b / 2 > 126e6 else
                           "state (%.3f GB) fits in the 126 MB L2: not a valid headline size" % (n * b / 1e9))}
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons of one GPU, sampled every 100 ms
+    while the context is open.  The GPU is named by its UUID (torch's device
+    index need not be nvidia-smi's index under CUDA_VISIBLE_DEVICES); entering
+    waits until the first sample is written, because nvidia-smi takes about a
+    second to start and a short timed region would otherwise see none."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+        self.gpu = str(gpu_index)
+        try:
+            import torch
+            self.gpu = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:  # noqa: BLE001 -- fall back to the index
+            pass
         self.proc = None
         self.path = None
 
@@ -160,10 +248,15 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+        t0 = time.monotonic()
+        while self.proc is not None and time.monotonic() - t0 < 15.0:
+            if self.proc.poll() is not None or os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
@@ -218,16 +311,29 @@ def run_ours(args, rank, local, world):
     tuning = s.tuning
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    barrier(world)
+    # steps per second of steady stepping before and after the timed steps, so
+    # that the clock samples describe the GPU under this load
+    e0.record(stream)
+    s.step(3)
+    e1.record(stream)
     torch.cuda.synchronize()
+    per_step = max(e0.elapsed_time(e1) / 3, 1e-3)
+    soak_before, soak_after = max(1, int(1000.0 / per_step)), max(1, int(300.0 / per_step))
     with ClockSampler(local) as clk:
+        s.step(soak_before)
+        barrier(world)
+        torch.cuda.synchronize()
         e0.record(stream)
         s.step(args.steps)
         e1.record(stream)
         torch.cuda.synchronize()
-    barrier(world)
+        barrier(world)
+        s.step(soak_after)
+        torch.cuda.synchronize()
     ms = allmax(e0.elapsed_time(e1), world)
     clocks = clk.summary()
+    clocks["window"] = (f"{soak_before} steps before the {args.steps} timed steps and {soak_after} after, "
+                        "sampled every 100 ms")
     ms_step = ms / args.steps
     value = weak_scaling_value(N, args.steps, ms, world)
     # the step kernel is the only launch per step (with obstacles the small
@@ -280,6 +386,52 @@ def run_ours(args, rank, local, world):
                    "uploaded once and copy_print read back once per run, the reference's stamp = nsteps cadence"}
     return {"value": value, "ms": ms, "ms_step": ms_step, "achieved": achieved, "clocks": clocks, "e2e": e2e,
             "finite": ok, "tuning": {"tile": [32, tuning[0]], "zseg": tuning[1]}}
+
+
+def measure_extra(kind: str, storage: str, L: int, steps: int, warmup: int, peak: float):
+    """Device-resident MLUPS and roofline of one more configuration on this
+    GPU, timed like the headline (CUDA events on the launching stream,
+    warm-up first; every state here is larger than the L2)."""
+    import numpy as np
+    import torch
+
+    import lbfast_b200 as lbf
+    stream = torch.cuda.current_stream()
+    t_setup = time.monotonic()
+    p, m, phi, isf = workload(storage, L, kind)
+    N = p.lx * p.ly * p.lz
+    s = lbf.Solver(p)
+    s.set_stream(stream.cuda_stream)
+    if isf is not None:
+        s.set_isfluid(isf)
+    s.set_fields(m, phi)
+    del m, phi
+    s.step(warmup)
+    s.sync()
+    t_setup = time.monotonic() - t_setup
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ms_step = ms / steps
+    b = bytes_per_lup(storage, kind) * N
+    try:
+        ok = bool(np.all(np.isfinite(s.reduce())))
+    except lbf.LbfError:
+        ok = False
+    tuning = s.tuning
+    s.close()
+    torch.cuda.empty_cache()
+    achieved = b / (ms_step * 1e-3) / 1e9
+    return {"config": config_dict(storage, L, kind), "value": N * steps / (ms * 1e-3) / 1e6, "unit": UNIT,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms_step,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "bytes_per_launch": b},
+            "launch": {"tile": [32, tuning[0]], "zseg": tuning[1]}, "finite": ok, "setup_s": t_setup}
 
 
 # ---- serving: an ensemble of droplet solves of uneven box sizes ----------
@@ -421,10 +573,11 @@ def run_serving(n: int, nsteps: int, seed: int = 7):
 
 def cpu_baseline(storage: str, L: int, nsteps: int, threads: int, kind: str = "laplace", warmup: int = 0):
     """The oracle (C restatement of the reference, FP32 build stand-in) on the
-    host cores: `warmup` untimed steps, then `nsteps` timed steps of the same box."""
+    host cores: `warmup` untimed steps, then `nsteps` timed steps of the same
+    box, set up with the oracle's own helpers."""
     import numpy as np
     from oracle import oracle as O
-    p, m, phi, isf = workload(storage, L, kind)
+    p, m, phi, isf = workload(storage, L, kind, oracle_helpers=True)
     O.set_threads(threads)
     o = O.Oracle(p.oracle_dict(), "f32")
     o.set_isfluid(isf if isf is not None else np.ones(p.shape, np.int8))
@@ -454,6 +607,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-solves", type=int, default=40, help="solves of the serving measurement (0: skip)")
     ap.add_argument("--serve-steps", type=int, default=3000)
+    ap.add_argument("--extra", default="f16,channel,c4,c4f16",
+                    help="comma list of extra device-resident lines: f16 (FP16 storage, headline box), channel "
+                         "(512x256x256 FP32), c4 / c4f16 (768^3 seeded droplets, FP32 / FP16); '' for none")
+    ap.add_argument("--extra-steps", type=int, default=20)
+    ap.add_argument("--no-tg-baseline", action="store_true",
+                    help="skip the CPU Taylor-Green baseline (64^3 D3Q19, 1000 steps)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -472,7 +631,8 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": k, "warmup": args.warmup, "ms_per_step": dt / k * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_dict(args.storage, args.box, args.workload),
+                "config": dict(config_dict(args.storage, args.box, args.workload),
+                               parallelism=f"replicas x{args.gpus}"),
                 "cpu_baseline": {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
                                  "sample": f"{k} steps of the {box_of(args.workload, args.box)} box, FP32 C restatement of the "
                                            f"reference kernels (oracle/lbf_oracle.c), OpenMP over z"},
@@ -490,12 +650,27 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     r = run_ours(args, rank, local, world)
+    extra = []
+    if rank == 0 and world == 1:
+        table = {"f16": ("laplace", "f16", args.box), "channel": ("channel", "f32", args.box),
+                 "c4": ("droplets", "f32", 768), "c4f16": ("droplets", "f16", 768)}
+        for name in [x for x in args.extra.split(",") if x]:
+            kind, storage, L = table[name]
+            try:
+                extra.append(dict(measure_extra(kind, storage, L, args.extra_steps, args.warmup, peak), name=name))
+            except Exception as ex:  # noqa: BLE001 -- one failed extra line must not lose the headline
+                extra.append({"name": name, "error": f"{type(ex).__name__}: {ex}"})
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         mlups, dt = cpu_baseline(args.storage, args.box, args.cpu_steps, threads, args.workload)
         cpu = {"value": mlups, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{args.cpu_steps} steps of the same {box_of(args.workload, args.box)} box ({dt:.1f} s), FP32 C restatement of "
                          f"the reference kernels (oracle/lbf_oracle.c), OpenMP"}
+        if not args.no_tg_baseline:
+            tg, dt = cpu_baseline("f32", 64, 1000, threads, "taylorgreen")
+            cpu["taylor_green"] = {"value": tg, "unit": UNIT, "cores": threads, "kind": "port",
+                                   "sample": f"Taylor-Green 64^3 D3Q19 one component, the full 1000 steps ({dt:.1f} s), "
+                                             "FP32 oracle, OpenMP"}
     serving = None
     if rank == 0 and world == 1 and args.serve_solves > 0:
         serving = run_serving(args.serve_solves, args.serve_steps)
@@ -515,7 +690,7 @@ def main():
                      "bytes_per_launch": bytes_per_lup(args.storage, args.workload) * nbox[0] * nbox[1] * nbox[2]},
         "e2e": r["e2e"], "gpu_launches": args.steps * (2 if args.workload == "channel" else 1), "clocks": r["clocks"],
         "cpu_baseline": cpu,
-        "finite": r["finite"], "serving": serving,
+        "finite": r["finite"], "extra": extra, "serving": serving,
     }
     print(json.dumps(line))
     shutdown(world)

@@ -142,7 +142,7 @@ int autotune(lbf_handle* h) {
         if (it != g_tune_cache.end()) {
             h->tile_y = it->second.first;
             h->zseg = it->second.second;
-            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, h->tile_y);
+            h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), lbf::kernel_obs(h->p), h->tile_y);
             return LBF_OK;
         }
     }
@@ -170,7 +170,7 @@ int autotune(lbf_handle* h) {
     std::pair<int, int> pick(h->tile_y, h->zseg);
     int rc = LBF_OK;
     for (const auto& c : cand) {
-        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, c.first);
+        lbf::StepLauncher L = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), lbf::kernel_obs(h->p), c.first);
         if (!L) continue;
         lbf::StepArgs a;
         const int zs0 = h->zseg;
@@ -198,7 +198,7 @@ int autotune(lbf_handle* h) {
     if (rc) return rc;
     h->tile_y = pick.first;
     h->zseg = pick.second;
-    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), h->p.obstacles, h->tile_y);
+    h->launcher = lbf::step_launcher(h->storage, h->p.lattice, h->p.highorder, lbf::kernel_tc(h->p), lbf::kernel_obs(h->p), h->tile_y);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = pick;
     return LBF_OK;
@@ -265,7 +265,7 @@ int flush_wet(lbf_handle* h) {
 
 int prime(lbf_handle* h) {
     if (h->d_mass)
-        CUDA_TRY(lbf::launch_mass(h->storage, true, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass,
+        CUDA_TRY(lbf::launch_mass(h->storage, lbf::MASS_INITIAL, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass,
                                   h->stream));
     int rc = launch_wet(h, h->cur, 1 - h->cur, true);
     if (rc) return rc;
@@ -273,7 +273,7 @@ int prime(lbf_handle* h) {
     // the flux of the initial state (integrator_module.f90:179-182)
     if (h->d_mass && h->obc_open) {
         CUDA_TRY(launch_face_flux(h, h->cur));
-        CUDA_TRY(lbf::launch_mass(h->storage, false, h->N, h->phi[h->cur], h->isf, h->d_mass, h->stream));
+        CUDA_TRY(lbf::launch_mass(h->storage, lbf::MASS_APPLY, h->N, h->phi[h->cur], h->isf, h->d_mass, h->stream));
     }
     h->primed = true;
     return LBF_OK;
@@ -365,7 +365,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     // 16 rows do not fit in shared memory); tile_y = 0 also tunes the schedule
     h->tile_y = p->tile_y ? p->tile_y : (lbf::tile_available(p->storage, 16) ? 16 : 8);
     h->tuned = p->tile_y != 0;
-    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, lbf::kernel_tc(*p), p->obstacles, h->tile_y);
+    h->launcher = lbf::step_launcher(p->storage, p->lattice, p->highorder, lbf::kernel_tc(*p), lbf::kernel_obs(*p), h->tile_y);
     if (!h->launcher) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
@@ -776,6 +776,9 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press) {
         for (int f = 0; f < 3; ++f) a.su[f] = 1.0 / h->scale[lbf::NSCALE_H - 4 + f];
     }
     a.phi = h->tc ? h->phi[src] : nullptr;
+    // after a step, its sums of the input phi are still in d_mass
+    a.mass = h->step == 0 ? nullptr : h->d_mass;
+    a.isf = h->obs ? h->isf : nullptr;
     float* d = static_cast<float*>(h->staging);
     a.rho = rho ? d : nullptr;
     a.vel_out = vel ? d + N : nullptr;
@@ -823,6 +826,7 @@ void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u) {
     a.isf = h->obs ? h->isf : nullptr;
     a.err = h->d_err;
     a.rep = h->d_rep;
+    a.mass = h->d_mass;
     a.min = h->mom[in];
     a.mout = h->mom[out];
     a.uin = h->uold[in];
@@ -855,7 +859,17 @@ size_t handle_bytes(const lbf_params* p) {
 
 int handle_pre_step(lbf_handle* h) {
     int rc = launch_wet(h, h->cur, 1 - h->cur, false);
-    if (rc || !h->d_rep) return rc;
+    if (rc) return rc;
+    if (h->d_mass) {
+        // phi mass correction of this step's input phi (bcs_mesoscopic_phifields,
+        // integrator_module.f90:297): its sum and interface count, and the phi
+        // the input state carries through open faces; the step's kernels apply
+        // the correction where they read a node's phi
+        CUDA_TRY(launch_face_flux(h, h->cur));
+        CUDA_TRY(lbf::launch_mass(h->storage, lbf::MASS_SUM, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr,
+                                  h->d_mass, h->stream));
+    }
+    if (!h->d_rep) return LBF_OK;
     // REPULSIVE_FLUX force of this step from its input phi (integrator_module.f90:325-328)
     lbf::RepulsiveArgs a;
     a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
@@ -865,6 +879,7 @@ int handle_pre_step(lbf_handle* h) {
     a.phi = h->phi[h->cur];
     a.nrm = h->d_rnrm;
     a.force = h->d_rep;
+    a.mass = h->d_mass;
     CUDA_TRY(lbf::launch_repulsive(h->storage, a, h->stream));
     return LBF_OK;
 }
@@ -895,6 +910,7 @@ int handle_post_step(lbf_handle* h) {
         a.phi = h->tc ? h->phi[in] : nullptr;
         a.mom = h->mom[h->cur]; a.pres = h->pres[h->cur];
         for (int f = 0; f < lbf::NSCALE_H; ++f) a.scale[f] = h->scale[f];
+        a.mass = h->d_mass;
         if (h->nbb) CUDA_TRY(lbf::launch_bounce_back(h->storage, a, h->stream));
         for (int axis = 0; axis < 3; ++axis) {
             if (!(h->obc_open & (1 << axis))) continue;
@@ -907,9 +923,6 @@ int handle_post_step(lbf_handle* h) {
             }
         }
     }
-    if (!h->d_mass) return LBF_OK;
-    CUDA_TRY(launch_face_flux(h, h->cur));
-    CUDA_TRY(lbf::launch_mass(h->storage, false, h->N, h->phi[h->cur], h->obs ? h->isf : nullptr, h->d_mass, h->stream));
     return LBF_OK;
 }
 

@@ -38,6 +38,7 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.isf = a.isf;
     p.err = a.err;
     p.rep = static_cast<const R*>(a.rep);
+    p.mass = a.mass;
 }
 
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false, bool OBS = true>

@@ -27,6 +27,7 @@ struct StepArgs {
     const int8_t* isf;
     int* err;
     const void* rep;        // REPULSIVE_FLUX force of the step (3 x N, arithmetic type), or nullptr
+    const double* mass;     // phi mass correction: sums of the step's input phi (see launch_mass), or nullptr
 };
 
 using StepLauncher = cudaError_t (*)(const StepArgs&, cudaStream_t);
@@ -37,6 +38,9 @@ StepLauncher step_launcher(int storage, int lat, int ho, int tc, int obs, int ti
 // kernel class argument `tc` of a run: 0 one component, 1 two components,
 // 2 two components with REPULSIVE_FLUX (its own compilation of the step)
 inline int kernel_tc(const lbf_params& p) { return p.twocomponent ? (p.repulsive_flux ? 2 : 1) : 0; }
+// kernel class argument `obs`: the compilation with the obstacle code, which
+// also carries the phi mass correction of the step's input phi
+inline int kernel_obs(const lbf_params& p) { return (p.obstacles || p.phi_correction) ? 1 : 0; }
 bool tile_available(int storage, int tile_y);
 
 // Batched step of many boxes of one kernel class and tile height: fill writes
@@ -98,6 +102,8 @@ struct PrintArgs {
     float* rho;
     float* vel_out;      // interleaved 3 x N
     float* press;
+    const double* mass;  // phi mass correction of the printed step's input phi, or nullptr
+    const int8_t* isf;   // isfluid with obstacles, else nullptr (all fluid)
 };
 cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
 
@@ -117,12 +123,15 @@ cudaError_t launch_upload_pin(int storage, int src_dtype, long long N, const voi
 cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const double* inv_scale,
                                int c, void* dst, cudaStream_t st);
 
-// phi mass correction: initial == true stores the FP64 sum of phi over fluid
-// nodes in d_mass[2]; otherwise the sum and the count of 0.5 < phi < 0.9 go to
-// d_mass[0..1] and (d_mass[2] + d_mass[3] - sum) / count is added to those
-// nodes, d_mass[3] the open-face flux of the state (0 without open faces).
-// No host synchronisation (graph-capturable).
-cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
+// phi mass correction, d_mass = {sum, count, sum0, flux}.  MASS_INITIAL
+// stores the FP64 sum of phi over fluid nodes in d_mass[2]; MASS_SUM puts the
+// sum and the count of 0.5 < phi < 0.9 in d_mass[0..1] (the kernels of the
+// step then correct those nodes' values where they read them, see mass_corr);
+// MASS_APPLY also adds (d_mass[2] + d_mass[3] - sum) / count to those nodes in
+// memory (the pre-loop correction).  d_mass[3] is the open-face flux of the
+// state (0 without open faces).  No host synchronisation (graph-capturable).
+enum MassMode { MASS_INITIAL = 0, MASS_SUM = 1, MASS_APPLY = 2 };
+cudaError_t launch_mass(int storage, MassMode mode, long long N, void* phi, const int8_t* isf, double* d_mass,
                         cudaStream_t st);
 
 // Wall passes after a step, on the step's output moments, at isfluid = -1
@@ -153,6 +162,7 @@ struct BoundaryArgs {
     void* mom;                  // the step's output moments
     float* pres;                // the step's output P (16-bit storage)
     double scale[NSCALE_H];
+    const double* mass;         // phi mass correction of the step's input phi (see launch_mass), or nullptr
 };
 cudaError_t launch_open_face(int storage, const BoundaryArgs& a, cudaStream_t st);
 cudaError_t launch_bounce_back(int storage, const BoundaryArgs& a, cudaStream_t st);
@@ -172,6 +182,7 @@ struct RepulsiveArgs {
     const void* phi;            // the step's input phi
     double* nrm;                // 3 x N normals (work array)
     void* force;                // 3 x N force, arithmetic type of the storage
+    const double* mass;         // phi mass correction of the step's input phi (see launch_mass), or nullptr
 };
 cudaError_t launch_repulsive(int storage, const RepulsiveArgs& a, cudaStream_t st);
 

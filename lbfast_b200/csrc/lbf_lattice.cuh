@@ -130,6 +130,30 @@ template <> struct PhiStore<__nv_bfloat16> { using type = float; };
 enum : int { F_P = 0, F_U = 1, F_PXX = 4, F_UOLD = 10, F_PHI = 13, NSCALE = 14 };
 
 // ---------------------------------------------------------------------------
+// phi mass correction of a step's input phi (bcs_mesoscopic_phifields,
+// boundary_cds_module.f90:1864-1885, with apply_lagrangian_phi_kernel,
+// lb_cuda_boundary_module.f90:549-560).  m = {sum of the input phi over
+// fluid nodes, count of those with 0.5 < phi < 0.9, the initial sum, the phi
+// carried through open faces}, all FP64 in device memory.  The reference
+// corrects the input phi in place after compute_norm has read it, so the
+// gradient, normal and Laplacian of the step see the uncorrected values and
+// the moments, collision and phi update the corrected ones; the kernels here
+// leave phi in memory untouched and correct a node's value where those read it.
+// ---------------------------------------------------------------------------
+// correction per interface node, or false when there is none to apply
+__device__ __forceinline__ bool mass_corr(const double* m, double& corr) {
+    if (!m) return false;
+    const double cnt = m[1];
+    if (!(cnt > 0.0)) return false;
+    corr = (m[2] + m[3] - m[0]) / cnt;
+    return true;
+}
+// the corrected value of a fluid node, rounded to the storage type SP of phi
+template <typename SP> __device__ __forceinline__ double mass_corrected(double v, double corr) {
+    return (v > 0.5 && v < 0.9) ? (double)(SP)(v + corr) : v;
+}
+
+// ---------------------------------------------------------------------------
 // kernel parameters (by value)
 // ---------------------------------------------------------------------------
 template <typename S, typename R> struct StepParams {
@@ -152,6 +176,7 @@ template <typename S, typename R> struct StepParams {
     const int8_t* isf;  // N isfluid (obstacles), else nullptr
     int* err;         // device error word
     const R* rep;     // REPULSIVE_FLUX force (3 x N), else nullptr
+    const double* mass;  // phi mass correction of the input phi (see mass_corr), else nullptr
 };
 
 }  // namespace lbf

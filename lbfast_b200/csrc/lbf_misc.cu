@@ -197,6 +197,9 @@ __global__ void print_kernel(const PrintArgs a) {
     const SPres* P = static_cast<const SPres*>(a.P);
     const S* V = static_cast<const S*>(a.vel);
     const SP* ph = static_cast<const SP*>(a.phi);
+    // the copy_print of a step reads its input phi after the mass correction
+    double corr = 0.0;
+    const bool mc = mass_corr(a.mass, corr);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x) {
         R press = Codec<SPres>::ld(P, i, (R)a.sP);
         if (a.rho) {
@@ -204,6 +207,7 @@ __global__ void print_kernel(const PrintArgs a) {
             if (a.mode == 0) r = press;
             else {
                 R f = Codec<SP>::ld(ph, i, R(1));
+                if (mc && (!a.isf || a.isf[i] == 1 || a.isf[i] == -1)) f = (R)mass_corrected<SP>((double)f, corr);
                 r = a.mode == 1 ? f : (R)a.rho_r * f + (R(1) - f) * (R)a.rho_b;
             }
             a.rho[i] = (float)r;
@@ -406,15 +410,16 @@ __global__ void mass_apply_kernel(long long N, SP* phi, const int8_t* isf, const
     }
 }
 
-cudaError_t launch_mass(int storage, bool initial, long long N, void* phi, const int8_t* isf, double* d_mass,
+cudaError_t launch_mass(int storage, MassMode mode, long long N, void* phi, const int8_t* isf, double* d_mass,
                         cudaStream_t st) {
+    const bool initial = mode == MASS_INITIAL;
     cudaError_t e = cudaMemsetAsync(initial ? d_mass + 2 : d_mass, 0, (initial ? 1 : 2) * sizeof(double), st);
     if (e != cudaSuccess) return e;
     return by_storage(storage, [&](auto tag) {
         using SP = typename PhiStore<decltype(tag)>::type;
         SP* f = static_cast<SP*>(phi);
         mass_sum_kernel<SP><<<blocks_for(N, 256), 256, 0, st>>>(N, f, isf, initial ? d_mass + 2 : d_mass, !initial);
-        if (!initial) mass_apply_kernel<SP><<<blocks_for(N, 256), 256, 0, st>>>(N, f, isf, d_mass);
+        if (mode == MASS_APPLY) mass_apply_kernel<SP><<<blocks_for(N, 256), 256, 0, st>>>(N, f, isf, d_mass);
         return cudaGetLastError();
     });
 }

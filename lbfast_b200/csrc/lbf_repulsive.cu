@@ -69,10 +69,20 @@ template <typename SP, typename R> __global__ void rep_force_kernel(const Repuls
     const SP* ph = static_cast<const SP*>(a.phi);
     R* out = static_cast<R*>(a.force);
     const double eps = 1.0e-9;
+    // the pair search reads the step's input phi after the mass correction
+    // (thinfilm_scan_mark_cuda runs after bcs_mesoscopic_phifields,
+    // integrator_module.f90:297-328); the normals above are compute_norm's,
+    // from the uncorrected phi.  Every node of the search is a fluid node.
+    double corr = 0.0;
+    const bool mc = mass_corr(a.mass, corr);
+    auto PH = [&](long long i) {
+        const double v = (double)ph[i];
+        return mc ? mass_corrected<SP>(v, corr) : v;
+    };
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < N; g += (long long)gridDim.x * blockDim.x) {
         double fo[3] = {0, 0, 0};
         const int f = a.isf ? a.isf[g] : 1;
-        const double loc_phi = (double)ph[g];
+        const double loc_phi = (f == 1 || f == -1) ? PH(g) : (double)ph[g];
         double qloc = fmin(fmax(loc_phi, 0.0), 1.0);
         qloc = qloc * (1.0 - qloc);
         if ((f == 1 || f == -1) && qloc >= a.q_th) {
@@ -91,7 +101,7 @@ template <typename SP, typename R> __global__ void rep_force_kernel(const Repuls
                         const int fn = nb < 0 ? 1 : (a.isf ? a.isf[nb] : 1);
                         if (fn != 1 && fn != -1) continue;
                         const double r2 = (double)(di * di + dj * dj + dk * dk);
-                        double qn = nb < 0 ? 0.0 : (double)ph[nb];
+                        double qn = nb < 0 ? 0.0 : PH(nb);
                         qn = fmin(fmax(qn, 0.0), 1.0);
                         qn = qn * (1.0 - qn);
                         if (qn < a.q_th || fabs(qn - qloc) > 0.1 * fmax(qloc, 1.0e-12)) continue;
@@ -123,7 +133,7 @@ template <typename SP, typename R> __global__ void rep_force_kernel(const Repuls
                         nsx /= nsm; nsy /= nsm; nsz /= nsm;
                     }
                     if (dx * nsx + dy * nsy + dz * nsz < 0) { nsx = -nsx; nsy = -nsy; nsz = -nsz; }
-                    const double phi2 = nb < 0 ? 0.0 : (double)ph[nb];
+                    const double phi2 = nb < 0 ? 0.0 : PH(nb);
                     const double qpair = 0.5 * (q1 + phi2 * (1.0 - phi2));
                     const double qcl = fmin(fmax(qpair, eps), 0.25 - eps);
                     const double arg = 1.0 / (2.0 * sqrt(qcl));

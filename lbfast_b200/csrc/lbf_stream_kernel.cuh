@@ -131,18 +131,27 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             else nodeB = (r - 2 * R1X - TY + 1) * R1X + (R1X - 1);         // right column
         }
     }
-    auto r1_geom = [&](int node, int& off) -> bool {
+    // wrapped: the node was reached across a periodic face in x or y
+    auto r1_geom = [&](int node, int& off, bool& wrapped) -> bool {
+        wrapped = false;
         if (node < 0) { off = 0; return false; }
         int hx = node % R1X, hy = node / R1X;
         bool ok = true;
-        int gx = wrap_coord(X0 + hx - 1, nx, p.pbx, ok);
-        int gy = wrap_coord(Y0 + hy - 1, ny, p.pby, ok);
+        const int gx0 = X0 + hx - 1, gy0 = Y0 + hy - 1;
+        int gx = wrap_coord(gx0, nx, p.pbx, ok);
+        int gy = wrap_coord(gy0, ny, p.pby, ok);
+        wrapped = gx != gx0 || gy != gy0;
         off = ok ? gy * nx + gx : 0;
         return ok;
     };
     int offA, offB;
-    const bool okA = r1_geom(nodeA, offA);
-    const bool okB = r1_geom(nodeB, offB);
+    bool wrapA, wrapB;
+    const bool okA = r1_geom(nodeA, offA, wrapA);
+    const bool okB = r1_geom(nodeB, offB, wrapB);
+    // phi mass correction of the input phi (compiled with the obstacle code only)
+    double mcorr = 0.0;
+    bool do_mcorr = false;
+    if constexpr (OBS && TC) do_mcorr = mass_corr(p.mass, mcorr);
     const int ox = X0 + tx, oy = Y0 + ty;
     const bool out_ok = (ox < nx) && (oy < ny);
     const int out_off = oy * nx + ox;
@@ -475,6 +484,8 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     pxy += u * v; pxz += u * w; pyz += v * w;
                 }
                 R phi = 0, lap = 0, divt = 0, gfx = 0, gfy = 0, gfz = 0;
+                R phi_u = 0;         // phi before the mass correction
+                bool stale = false;  // the collision reads phi_u (see below)
                 if constexpr (TC) {
                     const int hx = node % R1X, hy = node / R1X;
                     const int c2 = (hy + 1) * R2X + (hx + 1);
@@ -495,6 +506,20 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                     gfx = g1[0 * R1N + node];
                     gfy = g1[1 * R1N + node];
                     gfz = g1[2 * R1N + node];
+                    if constexpr (OBS) {
+                        // from here on the input phi after the mass correction (the
+                        // gradient, theta and Laplacian above are compute_norm's, from
+                        // the uncorrected phi)
+                        if (do_mcorr) {
+                            phi_u = phi;
+                            phi = (R)mass_corrected<SP>((double)phi, mcorr);
+                            // a node reached across a periodic face is, in the
+                            // reference's fused kernel, a halo copy: its moments and
+                            // forces were exchanged after the moments kernel (corrected
+                            // phi), its phi before the correction
+                            stale = phi != phi_u && ((k ? wrapB : wrapA) || q < 0 || q >= nz);
+                        }
+                    }
                 }
                 // ---- moments prologue: lb_cuda_moments_module.f90:104-339 ----
                 R inv = R(1), mask = R(0), fxv, fyv, fzv;
@@ -594,6 +619,16 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                         const R phi_new = phi - u * R(0.5) * gfx - v * R(0.5) * gfy - w * R(0.5) * gfz +
                                           p.tau_diff * lap - p.sharp_c * divt;
                         CP::st(p.pout, gi, phi_new, p.scale[F_PHI]);
+                    }
+                }
+                if constexpr (OBS && TC) {
+                    if (stale) {
+                        // density and viscosity of the collision from the halo copy's
+                        // uncorrected phi (lb_cuda_fused_module.f90:590-620)
+                        const R rh = dr ? p.rho_r * phi_u + (R(1) - phi_u) * p.rho_b : R(1);
+                        if (dr) inv = rcp<R>(rh);
+                        visc_l = (p.rho_r * p.visc1 * phi_u + (R(1) - phi_u) * p.visc2 * p.rho_b) * inv;
+                        omega = rcp<R>(visc_l * R(3) + R(0.5));
                     }
                 }
                 // ---- collision: lb_cuda_fused_module.f90:531-713 ----

@@ -178,6 +178,10 @@ __device__ void node_state(const BoundaryArgs& a, int x, int y, int z, long long
 #pragma unroll 1
         for (int l = 0; l < 27; ++l) sw += WL<27>(l) * PHI(x + EX(l), y + EY(l), z + EZ(l));
         lap = 6.0 * (sw - phi);
+        // the moments, collision and phi update see the input phi after the
+        // mass correction; compute_norm above read it before (see mass_corr)
+        double corr;
+        if (mass_corr(a.mass, corr)) phi = mass_corrected<SP>(phi, corr);
     }
     // moments prologue (lb_cuda_moments_module.f90:104-339)
     double rhophi = 1.0, fxv = a.fx, fyv = a.fy, fzv = a.fz, grx = 0, gry = 0, grz = 0, mask = 0, cv = 0;

@@ -78,7 +78,7 @@ typedef struct orc_params {
     double visc1, visc2, rho_r, rho_b, sigma, width, tau_diff;
     double fx, fy, fz;
     double wettab_r;
-    int phi_correction; /* phi mass correction after every step (see mass_correction) */
+    int phi_correction; /* phi mass correction of every step's input phi (see mass_correction) */
     int smagorinsky;    /* SMAGORINSKI LES relaxation time (see smag_omega) */
     /* open boundaries (openbc = 1, INTERNAL_OBSTACLES): per axis x, y, z and
      * side (low, high) the openbc_type_x/y/z, openbc_press_x/y/z and
@@ -1225,10 +1225,15 @@ static double phi_sum_count(const orc_state *s, const real *ph, long *cnt)
  * corr = dphi / count added to every fluid node with 0.5 < phi < 0.9.  The
  * reference applies it only with open boundaries, where the target is
  * sum0 + flux, flux the phi carried through the open faces (phi_flux) by the
- * step's moments; with periodic and wall boundaries it is zero.  The
- * reference corrects the input phi of a step after compute_norm; here the
- * output phi of every step is corrected, with the flux of the output moments
- * and phi -- the same quantities one call earlier. */
+ * step's input moments; with periodic and wall boundaries it is zero.  It
+ * runs inside bcs_mesoscopic_phifields on the step's INPUT phi, after
+ * compute_norm has read it and before div theta, the moments, the fused
+ * kernel and update_phi (integrator_module.f90:297, 315, 371): the
+ * gradient, normal and Laplacian of the step see the uncorrected phi, the
+ * rest the corrected one.  Only interior nodes are written (the kernel's
+ * grid covers the interior tiles), so the periodic halo copy of phi keeps
+ * the uncorrected values until the next exchange -- which the fused
+ * kernel's halo ring reads. */
 static void mass_correction(orc_state *s, real *ph, double flux)
 {
     long cnt = 0;
@@ -1280,6 +1285,10 @@ static void one_step(orc_state *s)
             wetting(s, pA);
             if (s->p.openbc) open_phi_copy(s, pA);
         }
+        /* bcs_mesoscopic_phifields: the mass correction of the input phi
+         * (integrator_module.f90:297), no halo exchange after it */
+        if (s->p.phi_correction)
+            mass_correction(s, pA, s->p.obstacles && s->p.openbc ? phi_flux(s, A, pA) : 0.0);
         compute_div_theta(s);
         if (s->p.repulsive) repulsive(s, pA);
     }
@@ -1295,11 +1304,7 @@ static void one_step(orc_state *s)
         if (!s->p.bounce_back) obstacle_bb(s, A, B, pA);
         if (s->p.openbc) open_bc(s, A, B, pA);
     }
-    if (s->p.twocomp) {
-        if (s->p.phi_correction)
-            mass_correction(s, pB, s->p.obstacles && s->p.openbc ? phi_flux(s, B, pB) : 0.0);
-        halo_real(s, pB);
-    }
+    if (s->p.twocomp) halo_real(s, pB);
     s->flip = out;
     s->step++;
 }
