@@ -176,6 +176,45 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press);
  * the check a driver calls every few steps to stop a run that blew up. */
 int lbf_reduce(lbf_handle* h, double out[5]);
 
+/* ---- z slabs: one box split over several handles / GPUs ----
+ * Replaces the reference's MPI decomposition of the box and its halo
+ * exchange (mpi_module.f90:2203-3650: exchange_hfields/phifields/auxfields/
+ * forces_sendrecv, packed per direction at :2991-3210) for a split along z of
+ * a box periodic in z.  lbf_create_slab makes a handle on planes [z0, z1) of
+ * the box in `global` (at least 3 planes) with 3 halo planes on each side;
+ * its fields (lbf_set_isfluid, lbf_set_fields, lbf_get_fields) are the
+ * slab's box of z1 - z0 + 6 planes, halo planes included.  lbf_step advances
+ * the slab's own planes from the current halo planes.  Between steps the
+ * halos are refilled: lbf_slabs_exchange copies them between the slabs of
+ * one process (a periodic ring, slabs[i] above slabs[i-1]; peer copies when
+ * the slabs are on different GPUs), or the caller copies the regions of
+ * lbf_slab_region across processes (NCCL send/recv): for side 0 (low z) / 1
+ * (high z) and recv 0 / 1, the device address and byte count of the 3 planes
+ * of field `field` (0 .. lbf_slab_nregions - 1) of the current time level
+ * that a neighbour receives / that this slab receives; a side-1 send region
+ * goes to the side-0 receive region of the slab above.  Call the exchange
+ * also once after the first lbf_step(h, 0), which applies the pre-loop
+ * wetting.  Every node's arithmetic is the single box's: the slabs together
+ * give its bits.  Not for phi_correction, repulsive_flux or openbc (box-wide
+ * sums and windows) -> LBF_E_UNSUPPORTED; lbf_reduce of a slab too. */
+int lbf_create_slab(const lbf_params* global, int z0, int z1, lbf_handle** h);
+int lbf_slab_nregions(lbf_handle* h, int* n);
+int lbf_slab_region(lbf_handle* h, int side, int recv, int field, void** ptr, size_t* bytes);
+int lbf_slabs_exchange(lbf_handle* const* slabs, int n);
+
+/* ---- full-state checkpoint ----
+ * No counterpart in the reference, whose restart (lbf_write_restart_raw) is
+ * one time level in float32 and so resumes a run only approximately.  The
+ * checkpoint holds every stored field of both time levels in the storage
+ * precision, the wetting ghost values not yet written, the phi
+ * mass-correction sums, the storage scales, the step count and the
+ * time-level index; a run resumed from it continues bit for bit.
+ * lbf_read_checkpoint needs a handle created with the same parameters (and,
+ * with obstacles, the same isfluid set first); it returns LBF_E_ARG for a
+ * checkpoint of another box, storage or configuration. */
+int lbf_write_checkpoint(lbf_handle* h, const char* path);
+int lbf_read_checkpoint(lbf_handle* h, const char* path);
+
 /* ---- allocation-free reduction ----
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory while they run: a Fortran integrator whose device
@@ -264,16 +303,25 @@ int lbf_read_restart_raw(const char* dir, int lx, int ly, int lz, float* mom10, 
 
 /* VTK ImageData writer of print_vtk_sync (print_module.f90:22-244, 2789-2814):
  * <dir>/out_rho_NNNNNN.vti, out_vel_... (3 components), and out_press_... when
- * press is not NULL, byte for byte in the reference's layout (Float32 data;
- * the reference's PRINTHALF UnsignedShort variant is not provided). */
+ * press is not NULL, byte for byte in the reference's layout (Float32 data). */
 int lbf_write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
                   const float* press);
+/* The same files in the reference's PRINTHALF layout (print_module.f90:110-121,
+ * mpi_module.f90:3737-3842): the values rounded to IEEE binary16 (round to
+ * nearest even), declared DataArray type="UnsignedShort". */
+int lbf_write_vtk_half(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                       const float* press);
 
 /* raw + XDMF writer of print_raw_sync (print_module.f90:2007-2180): writes
  * <dir>/out_rho_NNNNNN.raw/.xdmf, out_vel_..., and out_press_... when press
  * is not NULL. */
 int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
                        const float* press);
+/* The same files in the reference's PRINTHALF layout (print_module.f90:2053-2164):
+ * binary16 bit patterns (round to nearest even), XDMF NumberType="UInt"
+ * Precision="2". */
+int lbf_write_raw_xdmf_half(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                            const float* press);
 
 /* ---------------------------------------------------------------------------
  * Batched solve server (no counterpart in the reference, which runs one box

@@ -28,7 +28,9 @@ EXPORTED = (
     "lbf_reduce", "lbf_mark_isfluid", "lbf_seed_solid_phi", "lbf_ic_taylor_green", "lbf_ic_droplet", "lbf_ic_lamb",
     "lbf_write_raw_xdmf", "lbf_server_create", "lbf_server_destroy", "lbf_server_submit", "lbf_server_run",
     "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning", "lbf_write_restart_raw",
-    "lbf_read_restart_raw", "lbf_write_vtk",
+    "lbf_read_restart_raw", "lbf_write_vtk", "lbf_write_vtk_half", "lbf_write_raw_xdmf_half",
+    "lbf_write_checkpoint", "lbf_read_checkpoint", "lbf_create_slab", "lbf_slab_nregions", "lbf_slab_region",
+    "lbf_slabs_exchange",
 )
 SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -93,6 +95,12 @@ def load() -> C.CDLL:
     lib.lbf_get_tuning.argtypes = [vp, P(C.c_int), P(C.c_int)]
     lib.lbf_get_print_fields.argtypes = [vp, fp, fp, fp]
     lib.lbf_reduce.argtypes = [vp, dp]
+    lib.lbf_create_slab.argtypes = [P(LbfParams), C.c_int, C.c_int, P(vp)]
+    lib.lbf_slab_nregions.argtypes = [vp, P(C.c_int)]
+    lib.lbf_slab_region.argtypes = [vp, C.c_int, C.c_int, C.c_int, P(vp), P(C.c_size_t)]
+    lib.lbf_slabs_exchange.argtypes = [P(vp), C.c_int]
+    lib.lbf_write_checkpoint.argtypes = [vp, C.c_char_p]
+    lib.lbf_read_checkpoint.argtypes = [vp, C.c_char_p]
     lib.lbf_mark_isfluid.argtypes = [C.c_int] * 8 + [i8p, i8p]
     lib.lbf_seed_solid_phi.argtypes = [C.c_int] * 4 + [i8p, dp]
     lib.lbf_ic_taylor_green.argtypes = [C.c_int] * 3 + [C.c_double, dp]
@@ -100,6 +108,8 @@ def load() -> C.CDLL:
     lib.lbf_ic_lamb.argtypes = [C.c_int] * 3 + [dp] + [C.c_double] * 5 + [C.c_int, i8p, dp, dp]
     lib.lbf_write_raw_xdmf.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
     lib.lbf_write_vtk.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    lib.lbf_write_raw_xdmf_half.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
+    lib.lbf_write_vtk_half.argtypes = [C.c_char_p] + [C.c_int] * 4 + [fp, fp, fp]
     lib.lbf_write_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, C.c_int, C.c_int]
     lib.lbf_read_restart_raw.argtypes = [C.c_char_p] + [C.c_int] * 3 + [fp, fp, P(C.c_int), P(C.c_int)]
     lib.lbf_server_create.argtypes = [P(LbfServerConfig), P(vp)]
@@ -290,6 +300,16 @@ class Solver:
                                             _ptr(press, C.c_float)))
         return rho, np.moveaxis(vel, -1, 0), press
 
+    def write_checkpoint(self, path: str) -> None:
+        """Full state of the run (both time levels in the storage precision),
+        from which read_checkpoint resumes it bit for bit."""
+        check(self.lib.lbf_write_checkpoint(self.h, str(path).encode()))
+
+    def read_checkpoint(self, path: str) -> None:
+        """Resume from write_checkpoint's file (same parameters; with obstacles
+        call set_isfluid first)."""
+        check(self.lib.lbf_read_checkpoint(self.h, str(path).encode()))
+
     def reduce(self) -> np.ndarray:
         out = np.zeros(5, dtype=np.float64)
         check(self.lib.lbf_reduce(self.h, _ptr(out, C.c_double)))
@@ -445,20 +465,22 @@ def read_restart_raw(directory: str, lx: int, ly: int, lz: int, twocomponent: bo
     return m, p, fr.value, fr2.value
 
 
-def write_vtk(directory: str, iframe: int, rho, vel, press=None) -> None:
-    """VTK ImageData files of the reference's print_vtk_sync."""
+def write_vtk(directory: str, iframe: int, rho, vel, press=None, half: bool = False) -> None:
+    """VTK ImageData files of the reference's print_vtk_sync (half: its
+    PRINTHALF layout, binary16 values)."""
     lz, ly, lx = rho.shape
     r = np.ascontiguousarray(rho, dtype=np.float32)
     v = np.ascontiguousarray(np.moveaxis(vel, 0, -1), dtype=np.float32)
     p = None if press is None else np.ascontiguousarray(press, dtype=np.float32)
-    check(load().lbf_write_vtk(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float), _ptr(v, C.c_float),
-                               _ptr(p, C.c_float)))
+    f = load().lbf_write_vtk_half if half else load().lbf_write_vtk
+    check(f(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float), _ptr(v, C.c_float), _ptr(p, C.c_float)))
 
 
-def write_raw_xdmf(directory: str, iframe: int, rho, vel, press=None) -> None:
+def write_raw_xdmf(directory: str, iframe: int, rho, vel, press=None, half: bool = False) -> None:
+    """raw + XDMF files of the reference's print_raw_sync (half: PRINTHALF)."""
     lz, ly, lx = rho.shape
     r = np.ascontiguousarray(rho, dtype=np.float32)
     v = np.ascontiguousarray(np.moveaxis(vel, 0, -1), dtype=np.float32)
     p = None if press is None else np.ascontiguousarray(press, dtype=np.float32)
-    check(load().lbf_write_raw_xdmf(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float),
-                                    _ptr(v, C.c_float), _ptr(p, C.c_float)))
+    f = load().lbf_write_raw_xdmf_half if half else load().lbf_write_raw_xdmf
+    check(f(directory.encode(), int(iframe), lx, ly, lz, _ptr(r, C.c_float), _ptr(v, C.c_float), _ptr(p, C.c_float)))

@@ -210,7 +210,7 @@ cudaError_t launch_face_flux(lbf_handle* h, int b) {
     if (!h->obc_open || !h->tc) return cudaSuccess;
     double inv[4];
     for (int f = 0; f < 4; ++f) inv[f] = 1.0 / h->scale[f];
-    return lbf::launch_phi_flux(h->storage, h->nx, h->ny, h->nz, h->obc_open, h->mom[b], h->phi[b], h->isf, inv,
+    return lbf::launch_phi_flux(h->storage, h->nx, h->ny, h->nz, h->obc_open, h->mom[b], h->pres[b], h->phi[b], h->isf, inv,
                                 h->d_mass + 3, h->stream);
 }
 
@@ -373,10 +373,11 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : 0;  // 0: persistent schedule
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
-        ok = ok && cudaMalloc(&h->mom[b], 10 * h->N * h->esz) == cudaSuccess;
+        // 16-bit storage: Pi - u u (6 fields) in 16 bits, P, u, v, w in FP32 (pres)
+        ok = ok && cudaMalloc(&h->mom[b], (is_half(h->storage) ? 6 : 10) * h->N * h->esz) == cudaSuccess;
         ok = ok && cudaMalloc(&h->uold[b], 3 * h->N * h->esz) == cudaSuccess;
         if (h->tc) ok = ok && cudaMalloc(&h->phi[b], h->N * h->psz) == cudaSuccess;
-        if (is_half(h->storage)) ok = ok && cudaMalloc(&h->pres[b], h->N * sizeof(float)) == cudaSuccess;
+        if (is_half(h->storage)) ok = ok && cudaMalloc(&h->pres[b], 4 * h->N * sizeof(float)) == cudaSuccess;
     }
     if (ok && h->obs) ok = cudaMalloc(&h->isf, h->N) == cudaSuccess;
     if (ok) ok = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
@@ -390,7 +391,7 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
     if (!ok) {
         cudaGetLastError();
         free_all(h);
-        size_t need = 2 * (13 * h->N * h->esz + (h->tc ? h->N * h->psz : 0)) + (h->obs ? h->N : 0);
+        size_t need = lbf::handle_bytes(p);
         delete h;
         return fail(LBF_E_NOMEM, "device allocation of %.3f GB failed", need / 1e9);
     }
@@ -430,7 +431,10 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
     if (h->p.bounce_back) {
         // BOUNCE_BACK: the nodes whose wall links the half-way bounce-back rewrites
         std::vector<long long> nb;
-        for (long long i = 0; i < h->N; ++i)
+        const long long plane = (long long)h->nx * h->ny;
+        const long long i_lo = h->slab ? lbf::SLAB_HALO * plane : 0;
+        const long long i_hi = h->slab ? (lbf::SLAB_HALO + h->nzs) * plane : h->N;
+        for (long long i = i_lo; i < i_hi; ++i)
             if (isf[i] == -1) nb.push_back(i);
         cudaFree(h->bb_nodes);
         h->bb_nodes = nullptr;
@@ -459,7 +463,12 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
     std::vector<long long> vs;
     std::vector<int> vd, vf, vsh;
     std::vector<double> vwn;
-    for (int k = 0; k < nz; ++k)
+    // a slab wets the solid nodes of its own planes only (its halo planes are
+    // the neighbours', copied with their ghost values), with the donor rules
+    // of the whole box: a donor below its first plane is skipped, one beyond
+    // its last plane is a wrapped donor
+    const int k_lo = h->slab ? lbf::SLAB_HALO : 0, k_hi = h->slab ? lbf::SLAB_HALO + h->nzs : nz;
+    for (int k = k_lo; k < k_hi; ++k)
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i) {
                 long long c = ((long long)k * ny + j) * nx + i;
@@ -491,9 +500,15 @@ int lbf_set_isfluid(lbf_handle* h, const int8_t* isf) {
                 if (bl < 0) continue;
                 int dc[3] = {i + EXh[bl], j + EYh[bl], k + EZh[bl]};
                 // the reference skips a donor on the low halo layer (local index 0)
-                if (dc[0] == -1 || dc[1] == -1 || dc[2] == -1) continue;
+                const int gz = h->slab ? h->zg0 + dc[2] - lbf::SLAB_HALO : dc[2];
+                if (dc[0] == -1 || dc[1] == -1 || gz == -1) continue;
                 int flag = lbf::WET_NORMAL;
                 for (int d = 0; d < 3; ++d) {
+                    if (h->slab && d == 2) {
+                        // the donor plane is in the slab's box; the whole box wraps it
+                        if (gz >= h->nzg && flag == lbf::WET_NORMAL) flag = lbf::WET_HIGHWRAP;
+                        continue;
+                    }
                     if (dc[d] >= dims[d]) {
                         if (!pb[d]) flag = lbf::WET_OUTSIDE;
                         else if (flag == lbf::WET_NORMAL) flag = lbf::WET_HIGHWRAP;
@@ -573,10 +588,10 @@ int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype)
     const bool half = h->storage == LBF_STORE_F16 || h->storage == LBF_STORE_BF16;
     int rc = LBF_OK;
     if (half) {
-        // 16-bit storage keeps Pi - u u (the deviation from equilibrium) with one
-        // power-of-two scale per group of fields (velocity, Pi - u u; P stays
-        // FP32): all ten fields are staged on the device, the group maxima and
-        // Pi - u u are computed there
+        // 16-bit storage keeps Pi - u u (the deviation from equilibrium) and
+        // u_old with one power-of-two scale per group of fields; P, u, v, w
+        // stay FP32: all ten fields are staged on the device, the group maxima
+        // and Pi - u u are computed there
         rc = ensure_staging(h, 10 * N * hb);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(h->staging, mom10, 10 * N * hb, cudaMemcpyHostToDevice, h->stream));
@@ -588,25 +603,25 @@ int lbf_set_fields(lbf_handle* h, const void* mom10, const void* phi, int dtype)
         float mU, mPi;
         std::memcpy(&mU, &bits[0], sizeof mU);
         std::memcpy(&mPi, &bits[1], sizeof mPi);
-        h->scale[0] = 1.0;
-        // velocity floor 1e-3: a flow that starts at rest keeps 11 significant
+        for (int f = 0; f < 4; ++f) h->scale[f] = 1.0;
+        // u_old floor 1e-3: a flow that starts at rest keeps 11 significant
         // bits down to ~1e-6 and still represents |u| up to 0.5, beyond any
         // lattice Boltzmann velocity
-        for (int f = 1; f <= 3; ++f) h->scale[f] = h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-3);
+        for (int f = 1; f <= 3; ++f) h->scale[lbf::NSCALE_H - 4 + f - 1] = pick_scale(h->storage, mU, 1e-3);
         for (int f = 4; f < 10; ++f) h->scale[f] = pick_scale(h->storage, mPi, 1e-4);
         for (int b = 0; b < 2; ++b) {
-            CUDA_TRY(lbf::launch_convert_in(h->storage, true, h->staging, dtype, h->pres[b], N, 1.0, h->stream));
-            for (int f = 1; f <= 3; ++f) {
+            for (int f = 0; f < 4; ++f) {
                 const char* src = static_cast<const char*>(h->staging) + f * N * hb;
-                char* dst = static_cast<char*>(h->mom[b]) + f * N * h->esz;
+                // FP32 P, u, v, w (the phi conversion converts to FP32 here)
+                CUDA_TRY(lbf::launch_convert_in(h->storage, true, src, dtype, h->pres[b] + f * N, N, 1.0, h->stream));
+                if (f == 0) continue;
                 char* udst = static_cast<char*>(h->uold[b]) + (f - 1) * N * h->esz;
-                CUDA_TRY(lbf::launch_convert_in(h->storage, false, src, dtype, dst, N, h->scale[f], h->stream));
                 CUDA_TRY(lbf::launch_convert_in(h->storage, false, src, dtype, udst, N,
                                                 h->scale[lbf::NSCALE_H - 4 + f - 1], h->stream));
             }
             for (int c = 0; c < 6; ++c)
                 CUDA_TRY(lbf::launch_upload_pin(h->storage, dtype, N, h->staging, c,
-                                                static_cast<char*>(h->mom[b]) + (4 + c) * N * h->esz, h->scale[4 + c],
+                                                static_cast<char*>(h->mom[b]) + c * N * h->esz, h->scale[4 + c],
                                                 h->stream));
         }
     } else {
@@ -714,12 +729,12 @@ int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype)
         for (int f = 0; f < lbf::NSCALE_H; ++f) inv[f] = 1.0 / h->scale[f];
         for (int f = 0; f < 10; ++f) {
             char* dst = static_cast<char*>(mom10) + f * N * hb;
-            if (f == 0 && half) {
-                rc = out_field(h->pres[h->cur], true, 1.0, mom10);
+            if (f < 4 && half) {
+                rc = out_field(h->pres[h->cur] + f * N, true, 1.0, dst);
             } else if (f >= 4 && half) {
                 // stored Pi - u u: the equilibrium part is added back on the device
-                CUDA_TRY(lbf::launch_download_pi(h->storage, dtype, N, h->mom[h->cur], inv, f - 4, h->staging,
-                                                  h->stream));
+                CUDA_TRY(lbf::launch_download_pi(h->storage, dtype, N, h->mom[h->cur], h->pres[h->cur] + N, inv,
+                                                  f - 4, h->staging, h->stream));
                 CUDA_TRY(cudaMemcpyAsync(dst, h->staging, N * hb, cudaMemcpyDeviceToHost, h->stream));
                 CUDA_TRY(cudaStreamSynchronize(h->stream));
             } else {
@@ -734,11 +749,16 @@ int lbf_get_fields(lbf_handle* h, void* mom10, void* phi, void* uold, int dtype)
     }
     if (uold) {
         for (int f = 0; f < 3; ++f) {
-            const void* src = (h->u_valid || h->step == 0)
-                                  ? static_cast<const char*>(h->uold[h->cur]) + f * N * h->esz
-                                  : static_cast<const char*>(h->mom[h->cur]) + (1 + f) * N * h->esz;
-            double sc = (h->u_valid || h->step == 0) ? h->scale[lbf::NSCALE_H - 4 + f] : h->scale[1 + f];
-            rc = out_field(src, false, 1.0 / sc, static_cast<char*>(uold) + f * N * hb);
+            char* dst = static_cast<char*>(uold) + f * N * hb;
+            if (h->u_valid || h->step == 0) {
+                rc = out_field(static_cast<const char*>(h->uold[h->cur]) + f * N * h->esz, false,
+                               1.0 / h->scale[lbf::NSCALE_H - 4 + f], dst);
+            } else if (is_half(h->storage)) {
+                rc = out_field(h->pres[h->cur] + (1 + f) * N, true, 1.0, dst);
+            } else {
+                rc = out_field(static_cast<const char*>(h->mom[h->cur]) + (1 + f) * N * h->esz, false,
+                               1.0 / h->scale[1 + f], dst);
+            }
             if (rc) return rc;
         }
     }
@@ -767,8 +787,10 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press) {
     a.rho_b = h->p.rho_b;
     a.P = is_half(h->storage) ? static_cast<const void*>(h->pres[src]) : h->mom[src];
     a.sP = 1.0 / h->scale[0];
+    a.vel32 = nullptr;
     if (h->step == 0) {
         a.vel = static_cast<const char*>(h->mom[h->cur]) + 1 * N * h->esz;
+        if (is_half(h->storage)) a.vel32 = h->pres[h->cur] + N;
         for (int f = 0; f < 3; ++f) a.su[f] = 1.0 / h->scale[1 + f];
     } else {
         if (!h->u_valid) return fail(LBF_E_STATE, "velocity of the last step was not kept");
@@ -794,6 +816,7 @@ int lbf_get_print_fields(lbf_handle* h, float* rho, float* vel, float* press) {
 int lbf_reduce(lbf_handle* h, double out[5]) {
     if (!h || !out) return fail(LBF_E_ARG, "lbf_reduce: null argument");
     if (!h->fields_set) return fail(LBF_E_STATE, "lbf_reduce before lbf_set_fields");
+    if (h->slab) return fail(LBF_E_UNSUPPORTED, "lbf_reduce of a slab: sum the slabs' fields (lbf_get_fields)");
     double inv[4];
     for (int f = 0; f < 4; ++f) inv[f] = 1.0 / h->scale[f];
     CUDA_TRY(lbf::launch_reduce(h->storage, h->N, h->mom[h->cur], h->pres[h->cur], h->tc ? h->phi[h->cur] : nullptr,
@@ -809,6 +832,241 @@ int lbf_reduce(lbf_handle* h, double out[5]) {
 
 }  // extern "C"
 
+// ---- z slabs of a larger box ----
+// A slab is a handle on planes [z0, z1) of a box periodic in z, with
+// SLAB_HALO planes on each side that hold copies of the neighbouring slabs'
+// planes.  Its step advances its own planes only; between steps the halos of
+// the current time level are refilled from the neighbours -- in one process
+// by lbf_slabs_exchange, across processes or GPUs by copying the regions
+// lbf_slab_region names (NCCL send/recv, peer copies).  Every node's
+// arithmetic is the single box's, so the slabs together give the single
+// box's bits.
+namespace {
+// field f of the current time level (f < nmom: the storage-type moments;
+// then the FP32 P, u, v, w of 16-bit storage; then u_old; then phi) and the
+// bytes of one of its planes
+bool slab_field(lbf_handle* h, int f, char** base, size_t* plane_bytes) {
+    const long long plane = (long long)h->nx * h->ny;
+    const int nmom = is_half(h->storage) ? 6 : 10, n32 = is_half(h->storage) ? 4 : 0;
+    const int c = h->cur;
+    if (f < nmom) {
+        *base = static_cast<char*>(h->mom[c]) + (size_t)f * h->N * h->esz;
+        *plane_bytes = plane * h->esz;
+    } else if (f < nmom + n32) {
+        *base = reinterpret_cast<char*>(h->pres[c] + (size_t)(f - nmom) * h->N);
+        *plane_bytes = plane * sizeof(float);
+    } else if (f < nmom + n32 + 3) {
+        *base = static_cast<char*>(h->uold[c]) + (size_t)(f - nmom - n32) * h->N * h->esz;
+        *plane_bytes = plane * h->esz;
+    } else if (f == nmom + n32 + 3 && h->tc) {
+        *base = static_cast<char*>(h->phi[c]);
+        *plane_bytes = plane * h->psz;
+    } else {
+        return false;
+    }
+    return true;
+}
+int slab_nfields(const lbf_handle* h) { return 13 + (h->tc ? 1 : 0); }
+}  // namespace
+
+extern "C" {
+
+int lbf_create_slab(const lbf_params* global, int z0, int z1, lbf_handle** out) {
+    if (!global || !out) return fail(LBF_E_ARG, "lbf_create_slab: null argument");
+    *out = nullptr;
+    if (!global->pbc_z) return fail(LBF_E_UNSUPPORTED, "lbf_create_slab: the box must be periodic in z");
+    if (z0 < 0 || z1 > global->lz || z1 - z0 < lbf::SLAB_HALO)
+        return fail(LBF_E_ARG, "lbf_create_slab: planes [%d, %d) of %d: a slab needs %d planes at least", z0, z1,
+                    global->lz, lbf::SLAB_HALO);
+    if (global->phi_correction || global->repulsive_flux || global->openbc)
+        return fail(LBF_E_UNSUPPORTED,
+                    "lbf_create_slab: phi_correction, repulsive_flux and openbc need box-wide data (not for slabs)");
+    lbf_params p = *global;
+    p.lz = (z1 - z0) + 2 * lbf::SLAB_HALO;
+    p.pbc_z = 0;  // the halo planes are real planes of the slab's box
+    int rc = lbf_create(&p, out);
+    if (rc) return rc;
+    lbf_handle* h = *out;
+    h->slab = true;
+    h->zg0 = z0;
+    h->nzs = z1 - z0;
+    h->nzg = global->lz;
+    return LBF_OK;
+}
+
+int lbf_slab_nregions(lbf_handle* h, int* n) {
+    if (!h || !n) return fail(LBF_E_ARG, "lbf_slab_nregions: null argument");
+    if (!h->slab) return fail(LBF_E_ARG, "lbf_slab_nregions: not a slab");
+    *n = slab_nfields(h);
+    return LBF_OK;
+}
+
+int lbf_slab_region(lbf_handle* h, int side, int recv, int field, void** ptr, size_t* bytes) {
+    if (!h || !ptr || !bytes) return fail(LBF_E_ARG, "lbf_slab_region: null argument");
+    if (!h->slab) return fail(LBF_E_ARG, "lbf_slab_region: not a slab");
+    if (side < 0 || side > 1 || field < 0 || field >= slab_nfields(h))
+        return fail(LBF_E_ARG, "lbf_slab_region: side %d / field %d out of range", side, field);
+    char* base;
+    size_t pb;
+    slab_field(h, field, &base, &pb);
+    const int H = lbf::SLAB_HALO;
+    // low side: send the first H own planes, receive into planes 0 .. H-1;
+    // high side: send the last H own planes, receive into the H planes after them
+    const int first = side == 0 ? (recv ? 0 : H) : (recv ? H + h->nzs : h->nzs);
+    *ptr = base + (size_t)first * pb;
+    *bytes = (size_t)H * pb;
+    return LBF_OK;
+}
+
+int lbf_slabs_exchange(lbf_handle* const* slabs, int n) {
+    if (!slabs || n < 1) return fail(LBF_E_ARG, "lbf_slabs_exchange: no slabs");
+    for (int i = 0; i < n; ++i) {
+        if (!slabs[i] || !slabs[i]->slab) return fail(LBF_E_ARG, "lbf_slabs_exchange: handle %d is not a slab", i);
+        if (slab_nfields(slabs[i]) != slab_nfields(slabs[0]) || slabs[i]->storage != slabs[0]->storage ||
+            slabs[i]->nx != slabs[0]->nx || slabs[i]->ny != slabs[0]->ny)
+            return fail(LBF_E_ARG, "lbf_slabs_exchange: slab %d does not match slab 0", i);
+    }
+    // every slab's step must be complete before its planes are copied
+    for (int i = 0; i < n; ++i) CUDA_TRY(cudaStreamSynchronize(slabs[i]->stream));
+    const int nf = slab_nfields(slabs[0]);
+    for (int i = 0; i < n; ++i) {
+        lbf_handle* lo = slabs[(i + n - 1) % n];  // the slab below (periodic ring)
+        lbf_handle* hi = slabs[(i + 1) % n];      // the slab above
+        for (int f = 0; f < nf; ++f) {
+            void *dst, *src;
+            size_t b, b2;
+            lbf_slab_region(slabs[i], 0, 1, f, &dst, &b);
+            lbf_slab_region(lo, 1, 0, f, &src, &b2);
+            CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, slabs[i]->stream));
+            lbf_slab_region(slabs[i], 1, 1, f, &dst, &b);
+            lbf_slab_region(hi, 0, 0, f, &src, &b2);
+            CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, slabs[i]->stream));
+        }
+    }
+    for (int i = 0; i < n; ++i) CUDA_TRY(cudaStreamSynchronize(slabs[i]->stream));
+    return LBF_OK;
+}
+
+}  // extern "C"
+
+// ---- full-state checkpoint ----
+// Every stored field of both time levels in the storage precision (moments,
+// the FP32 P, u, v, w of 16-bit storage, u_old, phi), the wetting ghost
+// values still waiting to be written, the mass-correction sums, the
+// per-field scales, the step count and the time-level index: a run resumed
+// from it continues bit for bit.  The file starts with a header that the
+// reader checks against the handle (box, storage, lattice and switches).
+namespace {
+constexpr char kCkptMagic[8] = {'L', 'B', 'F', 'C', 'K', 'P', 'T', '1'};
+struct CkptHeader {
+    char magic[8];
+    int32_t version, lx, ly, lz, storage, lattice, highorder, twocomponent, densratio, obstacles;
+    int32_t phi_correction, repulsive_flux, nwet, cur, primed, u_valid, wet_pending, wet_pending_target;
+    int64_t step;
+    double scale[lbf::NSCALE_H];
+};
+
+// the device regions of a handle that hold state, with their byte counts
+std::vector<std::pair<void*, size_t>> state_regions(lbf_handle* h) {
+    std::vector<std::pair<void*, size_t>> r;
+    const size_t N = (size_t)h->N;
+    const bool half = is_half(h->storage);
+    for (int b = 0; b < 2; ++b) {
+        r.emplace_back(h->mom[b], (half ? 6 : 10) * N * h->esz);
+        r.emplace_back(h->uold[b], 3 * N * h->esz);
+        if (h->tc) r.emplace_back(h->phi[b], N * h->psz);
+        if (half) r.emplace_back(h->pres[b], 4 * N * sizeof(float));
+        if (h->nwet > 0) r.emplace_back(h->wetW[b], (size_t)h->nwet * h->psz);
+    }
+    if (h->d_mass) r.emplace_back(h->d_mass, 4 * sizeof(double));
+    return r;
+}
+
+constexpr size_t kCkptChunk = size_t(64) << 20;
+}  // namespace
+
+extern "C" {
+
+int lbf_write_checkpoint(lbf_handle* h, const char* path) {
+    if (!h || !path) return fail(LBF_E_ARG, "lbf_write_checkpoint: null argument");
+    if (!h->fields_set) return fail(LBF_E_STATE, "lbf_write_checkpoint before lbf_set_fields");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CkptHeader hd;
+    std::memset(&hd, 0, sizeof hd);
+    std::memcpy(hd.magic, kCkptMagic, 8);
+    hd.version = 1;
+    hd.lx = h->nx; hd.ly = h->ny; hd.lz = h->nz;
+    hd.storage = h->storage; hd.lattice = h->p.lattice; hd.highorder = h->p.highorder;
+    hd.twocomponent = h->p.twocomponent; hd.densratio = h->p.densratio; hd.obstacles = h->p.obstacles;
+    hd.phi_correction = h->p.phi_correction; hd.repulsive_flux = h->p.repulsive_flux; hd.nwet = h->nwet;
+    hd.cur = h->cur; hd.primed = h->primed; hd.u_valid = h->u_valid;
+    hd.wet_pending = h->wet_pending; hd.wet_pending_target = h->wet_pending_target;
+    hd.step = h->step;
+    for (int i = 0; i < lbf::NSCALE_H; ++i) hd.scale[i] = h->scale[i];
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(LBF_E_IO, "lbf_write_checkpoint: cannot open %s", path);
+    bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1;
+    std::vector<char> buf;
+    cudaError_t e = cudaSuccess;
+    for (const auto& reg : state_regions(h)) {
+        for (size_t off = 0; ok && off < reg.second; off += kCkptChunk) {
+            const size_t n = std::min(kCkptChunk, reg.second - off);
+            buf.resize(n);
+            e = cudaMemcpy(buf.data(), static_cast<const char*>(reg.first) + off, n, cudaMemcpyDeviceToHost);
+            ok = e == cudaSuccess && std::fwrite(buf.data(), 1, n, f) == n;
+        }
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (e != cudaSuccess) return fail(LBF_E_CUDA, "lbf_write_checkpoint: %s", cudaGetErrorString(e));
+    return ok ? LBF_OK : fail(LBF_E_IO, "lbf_write_checkpoint: write to %s failed", path);
+}
+
+int lbf_read_checkpoint(lbf_handle* h, const char* path) {
+    if (!h || !path) return fail(LBF_E_ARG, "lbf_read_checkpoint: null argument");
+    if (h->obs && !h->isf_set) return fail(LBF_E_STATE, "obstacles: call lbf_set_isfluid before lbf_read_checkpoint");
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(LBF_E_IO, "lbf_read_checkpoint: cannot open %s", path);
+    CkptHeader hd;
+    bool ok = std::fread(&hd, sizeof hd, 1, f) == 1 && std::memcmp(hd.magic, kCkptMagic, 8) == 0 && hd.version == 1;
+    if (!ok) {
+        std::fclose(f);
+        return fail(LBF_E_IO, "lbf_read_checkpoint: %s is not a checkpoint of this library", path);
+    }
+    if (hd.lx != h->nx || hd.ly != h->ny || hd.lz != h->nz || hd.storage != h->storage ||
+        hd.lattice != h->p.lattice || hd.highorder != h->p.highorder || hd.twocomponent != h->p.twocomponent ||
+        hd.densratio != h->p.densratio || hd.obstacles != h->p.obstacles ||
+        hd.phi_correction != h->p.phi_correction || hd.repulsive_flux != h->p.repulsive_flux || hd.nwet != h->nwet) {
+        std::fclose(f);
+        return fail(LBF_E_ARG, "lbf_read_checkpoint: %s was written for another box, storage or configuration", path);
+    }
+    std::vector<char> buf;
+    cudaError_t e = cudaSuccess;
+    for (const auto& reg : state_regions(h)) {
+        for (size_t off = 0; ok && off < reg.second; off += kCkptChunk) {
+            const size_t n = std::min(kCkptChunk, reg.second - off);
+            buf.resize(n);
+            ok = std::fread(buf.data(), 1, n, f) == n;
+            if (ok) e = cudaMemcpy(static_cast<char*>(reg.first) + off, buf.data(), n, cudaMemcpyHostToDevice);
+            ok = ok && e == cudaSuccess;
+        }
+    }
+    if (ok) ok = std::fgetc(f) == EOF;  // nothing after the state
+    std::fclose(f);
+    if (e != cudaSuccess) return fail(LBF_E_CUDA, "lbf_read_checkpoint: %s", cudaGetErrorString(e));
+    if (!ok) return fail(LBF_E_IO, "lbf_read_checkpoint: %s is truncated or too long", path);
+    h->cur = hd.cur;
+    h->primed = hd.primed != 0;
+    h->u_valid = hd.u_valid != 0;
+    h->wet_pending = hd.wet_pending;
+    h->wet_pending_target = hd.wet_pending_target;
+    h->step = hd.step;
+    for (int i = 0; i < lbf::NSCALE_H; ++i) h->scale[i] = hd.scale[i];
+    h->fields_set = true;
+    return LBF_OK;
+}
+
+}  // extern "C"
+
 namespace lbf {
 
 int handle_prime(lbf_handle* h) { return h->primed ? LBF_OK : prime(h); }
@@ -818,6 +1076,8 @@ void handle_step_args(const lbf_handle* h, StepArgs& a, bool write_u) {
     a.nx = h->nx; a.ny = h->ny; a.nz = h->nz;
     a.pbx = h->p.pbc_x; a.pby = h->p.pbc_y; a.pbz = h->p.pbc_z;
     a.densratio = h->dr; a.obstacles = h->obs; a.zseg = h->zseg; a.smag = h->p.smagorinsky;
+    a.zlo = h->slab ? lbf::SLAB_HALO : 0;
+    a.zhi = h->slab ? lbf::SLAB_HALO + h->nzs : h->nz;
     a.omega = h->omega; a.visc1 = h->p.visc1; a.visc2 = h->p.visc2;
     a.rho_r = h->tc ? h->p.rho_r : 1.0; a.rho_b = h->tc ? h->p.rho_b : 1.0;
     a.beta = h->beta; a.kapp = h->kapp; a.sharp_c = h->sharp_c; a.tau_diff = h->p.tau_diff;
@@ -848,9 +1108,10 @@ size_t handle_bytes(const lbf_params* p) {
     const long long N = (long long)p->lx * p->ly * p->lz;
     const size_t esz = storage_bytes(p->storage), psz = phi_bytes(p->storage);
     const bool half = p->storage == LBF_STORE_F16 || p->storage == LBF_STORE_BF16;
-    size_t b = 2 * (13 * N * esz);
+    // per time level: the moments (16-bit storage: Pi - u u in 16 bits, P, u,
+    // v, w in FP32) and u_old
+    size_t b = half ? 2 * (9 * N * esz + 4 * N * sizeof(float)) : 2 * (13 * N * esz);
     if (p->twocomponent) b += 2 * N * psz;
-    if (half) b += 2 * N * sizeof(float);
     if (p->obstacles) b += N;
     if (p->phi_correction) b += 4 * sizeof(double);
     if (p->repulsive_flux) b += 3 * N * (sizeof(double) + (p->storage == LBF_STORE_F64 ? 8 : 4));

@@ -52,7 +52,18 @@ struct lbf_handle {
     double* d_rnrm = nullptr;  // REPULSIVE_FLUX: normals (3 x N, FP64)
     void* d_rep = nullptr;     // REPULSIVE_FLUX: force of the step (3 x N, arithmetic type)
     bool tuned = true;   // false until the autotuner ran (tile_y = 0 requested)
+    // z slab of a larger box (lbf_create_slab): the handle's box is the slab's
+    // nzs planes plus SLAB_HALO halo planes on each side, filled from the
+    // neighbouring slabs; zg0 is the slab's first plane in the global box of nzg
+    bool slab = false;
+    int zg0 = 0, nzs = 0, nzg = 0;
 };
+
+namespace lbf {
+// halo planes of a z slab on each side: the step's phase-field stencils reach
+// three planes (phi for the gradient of theta of the collision's neighbours)
+constexpr int SLAB_HALO = 3;
+}  // namespace lbf
 
 namespace lbf {
 // integrator pre-loop work (wetting) of a freshly filled handle

@@ -166,9 +166,47 @@ int lbf_ic_lamb(int lx, int ly, int lz, const double center[3], double radius, d
     return droplet(lx, ly, lz, center, radius, width, sigma, rho_r, rho_b, densratio, isfluid, m, phi, 0.5);
 }
 
-// print_raw_sync, print_module.f90:2007-2180 (float32 stream files + XDMF)
-int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
-                       const float* press) {
+}  // extern "C"
+
+namespace {
+// IEEE 754 binary32 -> binary16, round to nearest even (overflow to
+// infinity, NaN kept quiet): the value the reference's real(kind=2) print
+// arrays hold under PRINTHALF
+uint16_t float_to_half_rne(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, sizeof b);
+    const uint32_t sign = (b >> 16) & 0x8000u;
+    const uint32_t ex = (b >> 23) & 0xffu;
+    uint32_t man = b & 0x7fffffu;
+    if (ex == 0xffu) return (uint16_t)(sign | 0x7c00u | (man ? 0x200u | (man >> 13) : 0u));
+    const int e = (int)ex - 127 + 15;  // biased binary16 exponent
+    if (e >= 31) return (uint16_t)(sign | 0x7c00u);
+    if (e <= 0) {
+        // subnormal (or zero) in binary16: shift the full significand
+        if (e < -10) return (uint16_t)sign;
+        man |= 0x800000u;
+        const int shift = 14 - e;  // 24-bit significand -> 10-bit field
+        uint32_t h = man >> shift;
+        const uint32_t rem = man & ((1u << shift) - 1u), half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (h & 1u))) ++h;
+        return (uint16_t)(sign | h);
+    }
+    uint32_t h = ((uint32_t)e << 10) | (man >> 13);
+    const uint32_t rem = man & 0x1fffu;
+    if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;  // a carry into the exponent is correct
+    return (uint16_t)(sign | h);
+}
+
+std::vector<uint16_t> to_half(const float* d, long long n) {
+    std::vector<uint16_t> out((size_t)n);
+    for (long long i = 0; i < n; ++i) out[(size_t)i] = float_to_half_rne(d[i]);
+    return out;
+}
+
+// print_raw_sync, print_module.f90:2007-2180 (float32 stream files + XDMF;
+// PRINTHALF: binary16 bit patterns, declared UInt of precision 2)
+int write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                   const float* press, bool half) {
     if (!dir) return LBF_E_ARG;
     const long long N = (long long)lx * ly * lz;
     char num[16];
@@ -194,7 +232,13 @@ int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, cons
         std::string xdmf = std::string(dir) + "/" + base + ".xdmf";
         FILE* f = std::fopen(raw.c_str(), "wb");
         if (!f) return LBF_E_IO;
-        size_t w = std::fwrite(it.data, sizeof(float), (size_t)(N * it.ncomp), f);
+        size_t w;
+        if (half) {
+            const std::vector<uint16_t> h16 = to_half(it.data, N * it.ncomp);
+            w = std::fwrite(h16.data(), sizeof(uint16_t), h16.size(), f);
+        } else {
+            w = std::fwrite(it.data, sizeof(float), (size_t)(N * it.ncomp), f);
+        }
         std::fclose(f);
         if (w != (size_t)(N * it.ncomp)) return LBF_E_IO;
         f = std::fopen(xdmf.c_str(), "w");
@@ -210,17 +254,32 @@ int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, cons
         std::fprintf(f, "      </Geometry>\n\n");
         std::fprintf(f, "      <!-- %s field associated with the grid -->\n", it.attr);
         std::fprintf(f, "      <Attribute Name=\"%s\" AttributeType=\"%s\" Center=\"Node\">\n", it.name, it.attr);
+        const char* ntype = half ? "UInt" : "Float";
+        const int prec = half ? 2 : 4;
         if (it.ncomp == 1)
-            std::fprintf(f, "        <DataItem Format=\"Binary\" NumberType=\"Float\" Precision=\"4\" Dimensions=\"%d %d %d\" Endian=\"%s\">\n",
-                         lz, ly, lx, little ? "Little" : "Big");
+            std::fprintf(f, "        <DataItem Format=\"Binary\" NumberType=\"%s\" Precision=\"%d\" Dimensions=\"%d %d %d\" Endian=\"%s\">\n",
+                         ntype, prec, lz, ly, lx, little ? "Little" : "Big");
         else
-            std::fprintf(f, "        <DataItem Format=\"Binary\" NumberType=\"Float\" Precision=\"4\" Dimensions=\"%d %d %d 3\" Endian=\"%s\">\n",
-                         lz, ly, lx, little ? "Little" : "Big");
+            std::fprintf(f, "        <DataItem Format=\"Binary\" NumberType=\"%s\" Precision=\"%d\" Dimensions=\"%d %d %d 3\" Endian=\"%s\">\n",
+                         ntype, prec, lz, ly, lx, little ? "Little" : "Big");
         std::fprintf(f, "          %s.raw\n        </DataItem>\n      </Attribute>\n\n    </Grid>\n  </Domain>\n</Xdmf>\n",
                      base.c_str());
         std::fclose(f);
     }
     return LBF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lbf_write_raw_xdmf(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                       const float* press) {
+    return write_raw_xdmf(dir, iframe, lx, ly, lz, rho, vel, press, false);
+}
+
+int lbf_write_raw_xdmf_half(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                            const float* press) {
+    return write_raw_xdmf(dir, iframe, lx, ly, lz, rho, vel, press, true);
 }
 
 }  // extern "C"
@@ -484,7 +543,8 @@ std::string rjust(long long v, int w) {
     return s.size() >= (size_t)w ? s : std::string(w - s.size(), ' ') + s;
 }
 
-int write_vti(const std::string& path, const char* name8, int ncomp, int lx, int ly, int lz, const float* data) {
+int write_vti(const std::string& path, const char* name8, int ncomp, int lx, int ly, int lz, const float* data,
+              bool half) {
     const long long N = (long long)lx * ly * lz;
     const std::string ext = rjust(1, 6) + " " + rjust(lx, 6) + " " + rjust(1, 6) + " " + rjust(ly, 6) + " " +
                             rjust(1, 6) + " " + rjust(lz, 6);
@@ -499,9 +559,11 @@ int write_vti(const std::string& path, const char* name8, int ncomp, int lx, int
     h += field("  <ImageData WholeExtent=\"" + ext + "\">", 70);
     h += field("    <Piece Extent=\"" + ext + "\">", 63);
     h += field("      <PointData>", 18);
-    h += field(std::string("        <DataArray type=\"Float32\" Name=\"") + name8 + "\" NumberOfComponents=\"" +
-                   std::to_string(ncomp) + "\" format=\"appended\" offset=\"" + rjust(0, 12) + "\"/>",
-               115);
+    // PRINTHALF declares the binary16 bit patterns as UnsignedShort (a field of 121)
+    h += field(std::string("        <DataArray type=\"") + (half ? "UnsignedShort" : "Float32") + "\" Name=\"" + name8 +
+                   "\" NumberOfComponents=\"" + std::to_string(ncomp) + "\" format=\"appended\" offset=\"" +
+                   rjust(0, 12) + "\"/>",
+               half ? 121 : 115);
     h += field("      </PointData>", 19);
     h += field("    </Piece>", 13);
     h += field("  </ImageData>", 15);
@@ -510,27 +572,44 @@ int write_vti(const std::string& path, const char* name8, int ncomp, int lx, int
     const std::string foot = std::string("\n") + "  </AppendedData>\n" + "</VTKFile>\n";
     std::FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) return LBF_E_IO;
-    const int32_t nbytes = (int32_t)(ncomp * N * (long long)sizeof(float));
+    const int32_t nbytes = (int32_t)(ncomp * N * (long long)(half ? sizeof(uint16_t) : sizeof(float)));
     bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
     ok = ok && std::fwrite(&nbytes, sizeof nbytes, 1, f) == 1;
-    ok = ok && std::fwrite(data, sizeof(float), ncomp * N, f) == (size_t)(ncomp * N);
+    if (half) {
+        const std::vector<uint16_t> h16 = to_half(data, ncomp * N);
+        ok = ok && std::fwrite(h16.data(), sizeof(uint16_t), h16.size(), f) == h16.size();
+    } else {
+        ok = ok && std::fwrite(data, sizeof(float), ncomp * N, f) == (size_t)(ncomp * N);
+    }
     ok = ok && std::fwrite(foot.data(), 1, foot.size(), f) == foot.size();
     if (std::fclose(f) != 0) ok = false;
     return ok ? LBF_OK : LBF_E_IO;
 }
 }  // namespace
 
-int lbf_write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
-                  const float* press) {
+namespace {
+int write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+              const float* press, bool half) {
     if (!dir || !rho || !vel || lx < 1 || ly < 1 || lz < 1) return LBF_E_ARG;
     char num[16];
     std::snprintf(num, sizeof(num), "%06d", iframe < 0 ? 0 : (iframe > 999999 ? 999999 : iframe));
     std::string d = dir;
     if (!d.empty() && d.back() != '/') d += '/';
-    int rc = write_vti(d + "out_rho_" + num + ".vti", "rho     ", 1, lx, ly, lz, rho);
-    if (rc == LBF_OK) rc = write_vti(d + "out_vel_" + num + ".vti", "vel     ", 3, lx, ly, lz, vel);
-    if (rc == LBF_OK && press) rc = write_vti(d + "out_press_" + num + ".vti", "press   ", 1, lx, ly, lz, press);
+    int rc = write_vti(d + "out_rho_" + num + ".vti", "rho     ", 1, lx, ly, lz, rho, half);
+    if (rc == LBF_OK) rc = write_vti(d + "out_vel_" + num + ".vti", "vel     ", 3, lx, ly, lz, vel, half);
+    if (rc == LBF_OK && press) rc = write_vti(d + "out_press_" + num + ".vti", "press   ", 1, lx, ly, lz, press, half);
     return rc;
+}
+}  // namespace
+
+int lbf_write_vtk(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                  const float* press) {
+    return write_vtk(dir, iframe, lx, ly, lz, rho, vel, press, false);
+}
+
+int lbf_write_vtk_half(const char* dir, int iframe, int lx, int ly, int lz, const float* rho, const float* vel,
+                       const float* press) {
+    return write_vtk(dir, iframe, lx, ly, lz, rho, vel, press, true);
 }
 
 // ---- restart.raw (print_module.f90:1030-1474 and 1474-1677) ----

@@ -19,6 +19,8 @@ template <typename S, typename R> void make_params(const StepArgs& a, StepParams
     p.N = p.plane * a.nz;
     p.densratio = a.densratio; p.obstacles = a.obstacles; p.write_u = a.write_u; p.smag = a.smag;
     p.zseg = a.zseg;
+    p.zlo = a.zlo;
+    p.zhi = a.zhi;
     p.omega = (R)a.omega; p.visc1 = (R)a.visc1; p.visc2 = (R)a.visc2;
     p.rho_r = (R)a.rho_r; p.rho_b = (R)a.rho_b; p.beta = (R)a.beta; p.kapp = (R)a.kapp;
     p.sharp_c = (R)a.sharp_c; p.tau_diff = (R)a.tau_diff;
@@ -53,8 +55,10 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     }
     StepParams<S, R> p;
     make_params(a, p);
+    const int nzr = a.zhi - a.zlo;
+    if (nzr <= 0) return cudaSuccess;
     if (a.zseg > 0) {
-        dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (a.nz + a.zseg - 1) / a.zseg);
+        dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (nzr + a.zseg - 1) / a.zseg);
         stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<grid, TX * TYV, smem, st>>>(p);
         return cudaGetLastError();
     }
@@ -65,7 +69,7 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         if (resident < 1) return cudaErrorInvalidConfiguration;
     }
-    const long long W = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV) * a.nz;
+    const long long W = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV) * nzr;
     const int grid = persistent_grid(W, resident);
     stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<grid, TX * TYV, smem, st>>>(p);
     return cudaGetLastError();

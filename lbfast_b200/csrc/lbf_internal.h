@@ -14,6 +14,7 @@ constexpr int NSCALE_H = 14;
 struct StepArgs {
     int nx, ny, nz, pbx, pby, pbz;
     int densratio, obstacles, write_u, zseg, smag;
+    int zlo, zhi;           // the planes advanced (a slab: its interior planes)
     double omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     double scale[NSCALE_H];
     const void* min;
@@ -22,7 +23,7 @@ struct StepArgs {
     void* uout;
     const void* pin;
     void* pout;
-    const float* pres_in;   // P with 16-bit storage
+    const float* pres_in;   // P, u, v, w with 16-bit storage (4 x N)
     float* pres_out;
     const int8_t* isf;
     int* err;
@@ -96,7 +97,8 @@ struct PrintArgs {
     int mode;            // 0: P, 1: phi, 2: rho_phi
     double rho_r, rho_b;
     const void* P;       // moment field 0 (float array with 16-bit storage)
-    const void* vel;     // 3 consecutive velocity fields
+    const void* vel;     // 3 consecutive velocity fields (storage type)
+    const float* vel32;  // or, when not null, 3 consecutive FP32 velocity fields
     const void* phi;
     double sP, su[3];    // inverse scales
     float* rho;
@@ -108,6 +110,7 @@ struct PrintArgs {
 cudaError_t launch_print(int storage, const PrintArgs& a, cudaStream_t st);
 
 // FP64 reductions over fluid nodes: out[5] = {sum phi, sum P, sum u, sum v, sum w}
+// (16-bit storage: P, u, v, w from pres)
 cudaError_t launch_reduce(int storage, long long N, const void* mom, const float* pres, const void* phi,
                           const int8_t* isf, const double* inv_scale, double* d_out, cudaStream_t st);
 
@@ -119,9 +122,10 @@ cudaError_t launch_upload_maxabs(int src_dtype, long long N, const void* staged1
 cudaError_t launch_upload_pin(int storage, int src_dtype, long long N, const void* staged10, int c, void* dst,
                               double scale, cudaStream_t st);
 // 16-bit download: component c of Pi = (Pi - u u) + u u from the stored
-// fields (mom: the ten 16-bit fields, inv_scale per field) into dst (dst_dtype)
-cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const double* inv_scale,
-                               int c, void* dst, cudaStream_t st);
+// fields (mom: the six 16-bit Pi - u u fields, inv_scale per moment field;
+// vel32: the FP32 u, v, w) into dst (dst_dtype)
+cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const float* vel32,
+                               const double* inv_scale, int c, void* dst, cudaStream_t st);
 
 // phi mass correction, d_mass = {sum, count, sum0, flux}.  MASS_INITIAL
 // stores the FP64 sum of phi over fluid nodes in d_mass[2]; MASS_SUM puts the
@@ -156,11 +160,11 @@ struct BoundaryArgs {
     long long nnodes;
     const int8_t* isf;
     const void* min;            // the step's input moments
-    const float* pres_in;       // the step's input P (16-bit storage)
+    const float* pres_in;       // the step's input P, u, v, w (16-bit storage, 4 x N)
     const void* uin;            // the step's input u_old (DENSRATIO)
     const void* phi;            // the step's input phi (two components)
     void* mom;                  // the step's output moments
-    float* pres;                // the step's output P (16-bit storage)
+    float* pres;                // the step's output P, u, v, w (16-bit storage, 4 x N)
     double scale[NSCALE_H];
     const double* mass;         // phi mass correction of the step's input phi (see launch_mass), or nullptr
 };
@@ -170,8 +174,9 @@ cudaError_t launch_bounce_back(int storage, const BoundaryArgs& a, cudaStream_t 
 // phi carried through the open faces by a state (BCPHIFLUX,
 // boundary_cds_module.f90:1667-1861): sum over the isfluid = -1 nodes of the
 // planes next to the walls of +-u_n phi, into d_flux (set, not added)
-cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const void* phi,
-                            const int8_t* isf, const double* inv_scale, double* d_flux, cudaStream_t st);
+cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const float* pres,
+                            const void* phi, const int8_t* isf, const double* inv_scale, double* d_flux,
+                            cudaStream_t st);
 
 // REPULSIVE_FLUX before a step (lbf_repulsive.cu): the film-repulsion force
 // of every node from the step's input phi into `force`

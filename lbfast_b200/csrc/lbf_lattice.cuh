@@ -118,13 +118,30 @@ template <> struct Codec<__nv_bfloat16> {
     }
 };
 
-// phi and P keep 32-bit storage when the other moments are stored in 16 bits:
-// phi lives in [0,1] and a 16-bit mantissa cannot resolve its interface
-// profile; P is conserved, so its rounding errors add up step after step
-// instead of relaxing away as the velocity's and Pi's do.
+// phi, P and the velocity keep 32-bit storage when the other moments are
+// stored in 16 bits: phi lives in [0,1] and a 16-bit mantissa cannot resolve
+// its interface profile; P and u are carried from step to step (P is
+// conserved, u changes by the body force, ~1e-6 a step on ~1e-4 in a driven
+// channel), so a 16-bit rounding of them every step would add up instead of
+// relaxing away as the rounding of Pi - u u and of u_old (rewritten from the
+// 32-bit u every step) does.
 template <typename S> struct PhiStore { using type = S; };
 template <> struct PhiStore<__half> { using type = float; };
 template <> struct PhiStore<__nv_bfloat16> { using type = float; };
+
+// Where the ten moment fields live.  FP32 / FP64 storage: one array of
+// 10 x N in the storage type.  16-bit storage: P, u, v, w in an FP32 array of
+// 4 x N (`pres`), Pi - u u in the 16-bit array (6 x N, field f >= 4 at
+// (f - 4) x N).
+template <typename S> struct Layout {
+    static constexpr bool split = Codec<S>::scaled;
+    static constexpr int nmom = split ? 6 : 10;  // fields of the storage-type array
+    static constexpr int n32 = split ? 4 : 0;    // fields of the FP32 array
+    // offset of field f in the storage-type array (f >= 4 when split)
+    __host__ __device__ static constexpr long long off(int f, long long N) {
+        return split ? (long long)(f - 4) * N : (long long)f * N;
+    }
+};
 
 // field slots of the per-field scale table
 enum : int { F_P = 0, F_U = 1, F_PXX = 4, F_UOLD = 10, F_PHI = 13, NSCALE = 14 };
@@ -163,12 +180,13 @@ template <typename S, typename R> struct StepParams {
     long long N;      // nx*ny*nz
     int densratio, obstacles, write_u, smag;
     int zseg;         // planes per z segment
+    int zlo, zhi;     // the planes advanced: zlo <= z < zhi (0 and nz but for a slab)
     R omega, visc1, visc2, rho_r, rho_b, beta, kapp, sharp_c, tau_diff, fx, fy, fz;
     R scale[NSCALE], inv_scale[NSCALE];
-    const S* min;     // 10 x N moments, input (field 0 unused with 16-bit storage)
-    S* mout;          // 10 x N moments, output
-    const float* pres_in;  // N pressure moment P, input (16-bit storage only)
-    float* pres_out;       // N pressure moment P, output (16-bit storage only)
+    const S* min;     // moments, input (10 x N; 16-bit storage: Pi - u u, 6 x N, see Layout)
+    S* mout;          // moments, output
+    const float* pres_in;  // 4 x N: P, u, v, w, input (16-bit storage only)
+    float* pres_out;       // 4 x N: P, u, v, w, output (16-bit storage only)
     const S* uin;     // 3 x N velocity of the previous step (DENSRATIO)
     S* uout;          // 3 x N velocity after the force half-step
     const typename PhiStore<S>::type* pin;  // N phase field, input

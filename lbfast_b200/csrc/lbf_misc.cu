@@ -213,7 +213,11 @@ __global__ void print_kernel(const PrintArgs a) {
             a.rho[i] = (float)r;
         }
         if (a.press) a.press[i] = (float)press;
-        if (a.vel_out) {
+        if (a.vel_out && a.vel32) {
+            a.vel_out[3 * i + 0] = a.vel32[i];
+            a.vel_out[3 * i + 1] = a.vel32[a.N + i];
+            a.vel_out[3 * i + 2] = a.vel32[2 * a.N + i];
+        } else if (a.vel_out) {
             a.vel_out[3 * i + 0] = (float)Codec<S>::ld(V, i, (R)a.su[0]);
             a.vel_out[3 * i + 1] = (float)Codec<S>::ld(V, a.N + i, (R)a.su[1]);
             a.vel_out[3 * i + 2] = (float)Codec<S>::ld(V, 2 * a.N + i, (R)a.su[2]);
@@ -245,10 +249,17 @@ __global__ void reduce_kernel(long long N, const S* mom, const float* pres, cons
             if (f != 1 && f != -1) continue;
         }
         if (phi) acc[0] += (double)Codec<SP>::ld(phi, i, 1.0);
-        acc[1] += pres ? (double)pres[i] : (double)Codec<S>::ld(mom, i, s0);
-        acc[2] += (double)Codec<S>::ld(mom, N + i, s1);
-        acc[3] += (double)Codec<S>::ld(mom, 2 * N + i, s2);
-        acc[4] += (double)Codec<S>::ld(mom, 3 * N + i, s3);
+        if (Layout<S>::split) {
+            acc[1] += (double)pres[i];
+            acc[2] += (double)pres[N + i];
+            acc[3] += (double)pres[2 * N + i];
+            acc[4] += (double)pres[3 * N + i];
+        } else {
+            acc[1] += (double)Codec<S>::ld(mom, i, s0);
+            acc[2] += (double)Codec<S>::ld(mom, N + i, s1);
+            acc[3] += (double)Codec<S>::ld(mom, 2 * N + i, s2);
+            acc[4] += (double)Codec<S>::ld(mom, 3 * N + i, s3);
+        }
     }
     __shared__ double red[5][256];
 #pragma unroll
@@ -333,28 +344,29 @@ cudaError_t launch_upload_pin(int storage, int src_dtype, long long N, const voi
     return cudaErrorInvalidValue;
 }
 
+// vel32 holds u, v, w (FP32); moment field a in 1..3 is vel32[(a - 1) N]
 template <typename S, typename T>
-__global__ void download_pi_kernel(long long N, const S* m, float sa, float sb, float sc, int a, int b, int c, T* dst) {
+__global__ void download_pi_kernel(long long N, const S* m, const float* vel32, float sc, int a, int b, int c, T* dst) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        const double ua = (double)Codec<S>::ld(m + a * N, i, sa);
-        const double ub = (double)Codec<S>::ld(m + b * N, i, sb);
-        const double pn = (double)Codec<S>::ld(m + (4 + c) * N, i, sc);
+        const double ua = (double)vel32[(a - 1) * N + i];
+        const double ub = (double)vel32[(b - 1) * N + i];
+        const double pn = (double)Codec<S>::ld(m + c * N, i, sc);
         dst[i] = (T)(pn + ua * ub);
     }
 }
 
-cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const double* inv_scale,
-                               int c, void* dst, cudaStream_t st) {
+cudaError_t launch_download_pi(int storage, int dst_dtype, long long N, const void* mom, const float* vel32,
+                               const double* inv_scale, int c, void* dst, cudaStream_t st) {
     const int a = PIN_A[c], b = PIN_B[c];
     auto go = [&](auto stag) {
         using S = decltype(stag);
         const S* m = static_cast<const S*>(mom);
         if (dst_dtype == 1)
             download_pi_kernel<S, double><<<blocks_for(N, 256), 256, 0, st>>>(
-                N, m, (float)inv_scale[a], (float)inv_scale[b], (float)inv_scale[4 + c], a, b, c, static_cast<double*>(dst));
+                N, m, vel32, (float)inv_scale[4 + c], a, b, c, static_cast<double*>(dst));
         else
             download_pi_kernel<S, float><<<blocks_for(N, 256), 256, 0, st>>>(
-                N, m, (float)inv_scale[a], (float)inv_scale[b], (float)inv_scale[4 + c], a, b, c, static_cast<float*>(dst));
+                N, m, vel32, (float)inv_scale[4 + c], a, b, c, static_cast<float*>(dst));
         return cudaGetLastError();
     };
     if (storage == 1) return go(__half());

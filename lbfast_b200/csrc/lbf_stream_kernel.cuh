@@ -375,17 +375,23 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     // The tile-interior node's are loaded one plane ahead, at the start of the
     // pull phase of the plane before, so their latency passes behind that
     // phase and its barrier; the ring nodes load theirs at the point of use.
+    using LY = Layout<S>;
     struct NodeRaw {
-        S m[10];
-        float P;  // 32-bit P of the scaled formats (m[0] unused there)
+        S m[10];      // with 16-bit storage only m[4..9] (Pi - u u)
+        float v32[4];  // P, u, v, w of the 16-bit formats
         S uo[3];
         int8_t isf;
     };
     auto fetch = [&](int gi, NodeRaw& r) {
-        if constexpr (CD::scaled) r.P = __ldg(p.pres_in + gi);
-        else r.m[0] = CD::raw(p.min, gi);
+        if constexpr (LY::split) {
 #pragma unroll
-        for (int f = 1; f < 10; ++f) r.m[f] = CD::raw(p.min + f * N, gi);
+            for (int f = 0; f < 4; ++f) r.v32[f] = __ldg(p.pres_in + f * N + gi);
+#pragma unroll
+            for (int f = 4; f < 10; ++f) r.m[f] = CD::raw(p.min + LY::off(f, N), gi);
+        } else {
+#pragma unroll
+            for (int f = 0; f < 10; ++f) r.m[f] = CD::raw(p.min + f * N, gi);
+        }
         if (dr) {
 #pragma unroll
             for (int f = 0; f < 3; ++f) r.uo[f] = CD::raw(p.uin + f * N, gi);
@@ -467,11 +473,14 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             R sP = 0, spxx = 0, spyy = 0, spzz = 0, spxy = 0, spxz = 0, spyz = 0, som = 0;
             if (live) {
                 R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;
-                if constexpr (CD::scaled) P = (R)cur.P;
-                else P = CD::dec(cur.m[0], p.inv_scale[0]);
-                u = CD::dec(cur.m[1], p.inv_scale[1]);
-                v = CD::dec(cur.m[2], p.inv_scale[2]);
-                w = CD::dec(cur.m[3], p.inv_scale[3]);
+                if constexpr (LY::split) {
+                    P = (R)cur.v32[0]; u = (R)cur.v32[1]; v = (R)cur.v32[2]; w = (R)cur.v32[3];
+                } else {
+                    P = CD::dec(cur.m[0], p.inv_scale[0]);
+                    u = CD::dec(cur.m[1], p.inv_scale[1]);
+                    v = CD::dec(cur.m[2], p.inv_scale[2]);
+                    w = CD::dec(cur.m[3], p.inv_scale[3]);
+                }
                 pxx = CD::dec(cur.m[4], p.inv_scale[4]);
                 pyy = CD::dec(cur.m[5], p.inv_scale[5]);
                 pzz = CD::dec(cur.m[6], p.inv_scale[6]);
@@ -816,17 +825,19 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 am[4] -= am[1] * am[1]; am[5] -= am[2] * am[2]; am[6] -= am[3] * am[3];
                 am[7] -= am[1] * am[2]; am[8] -= am[1] * am[3]; am[9] -= am[2] * am[3];
             }
-            if constexpr (CD::scaled) p.pres_out[go] = (float)am[0];
-            else CD::st(p.mout + 0 * N, go, am[0], p.scale[0]);
-            CD::st(p.mout + 1 * N, go, am[1], p.scale[1]);
-            CD::st(p.mout + 2 * N, go, am[2], p.scale[2]);
-            CD::st(p.mout + 3 * N, go, am[3], p.scale[3]);
-            CD::st(p.mout + 4 * N, go, am[4] - third, p.scale[4]);
-            CD::st(p.mout + 5 * N, go, am[5] - third, p.scale[5]);
-            CD::st(p.mout + 6 * N, go, am[6] - third, p.scale[6]);
-            CD::st(p.mout + 7 * N, go, am[7], p.scale[7]);
-            CD::st(p.mout + 8 * N, go, am[8], p.scale[8]);
-            CD::st(p.mout + 9 * N, go, am[9], p.scale[9]);
+            if constexpr (LY::split) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) p.pres_out[f * N + go] = (float)am[f];
+            } else {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) CD::st(p.mout + f * N, go, am[f], p.scale[f]);
+            }
+            CD::st(p.mout + LY::off(4, N), go, am[4] - third, p.scale[4]);
+            CD::st(p.mout + LY::off(5, N), go, am[5] - third, p.scale[5]);
+            CD::st(p.mout + LY::off(6, N), go, am[6] - third, p.scale[6]);
+            CD::st(p.mout + LY::off(7, N), go, am[7], p.scale[7]);
+            CD::st(p.mout + LY::off(8, N), go, am[8], p.scale[8]);
+            CD::st(p.mout + LY::off(9, N), go, am[9], p.scale[9]);
         }
 #pragma unroll
         for (int i = 0; i < 10; ++i) {
@@ -842,16 +853,17 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 // CTAs per SM the kernel is compiled for: two of 256 threads, one of 512, one in FP64
 template <typename R, int TYV> constexpr int step_min_blocks() { return (sizeof(R) == 8 || TYV > 8) ? 1 : 2; }
 
-// Column-planes of a box for a tile of TYV rows, column index = by * gx + bx.
+// Column-planes of the planes zlo .. zlo + nzr - 1 of a box for a tile of
+// TYV rows, column index = by * gx + bx, plane fastest.
 template <int TYV, typename F>
-__device__ __forceinline__ void run_share(const int nx, const int ny, const int nz, long long s0, long long s1,
+__device__ __forceinline__ void run_share(const int nx, const int nzr, const int zlo, long long s0, long long s1,
                                           F&& body) {
     const int gx = (nx + TX - 1) / TX;
     while (s0 < s1) {
-        const long long col = s0 / nz;
-        const int z0 = (int)(s0 - col * nz);
-        const int z1 = (int)min((long long)nz, z0 + (s1 - s0));
-        body((int)(col % gx), (int)(col / gx), z0, z1);
+        const long long col = s0 / nzr;
+        const int z0 = (int)(s0 - col * nzr);
+        const int z1 = (int)min((long long)nzr, z0 + (s1 - s0));
+        body((int)(col % gx), (int)(col / gx), zlo + z0, zlo + z1);
         s0 += z1 - z0;
     }
 }
@@ -868,18 +880,19 @@ __device__ __forceinline__ void run_share(const int nx, const int ny, const int 
 template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP = false, bool OBS = true>
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
     long long s0, s1;
+    const int nzr = p.zhi - p.zlo;
     if (p.zseg > 0) {
         const long long col = (long long)blockIdx.y * ((p.nx + TX - 1) / TX) + blockIdx.x;
         const int z0 = blockIdx.z * p.zseg;
-        s0 = col * p.nz + z0;
-        s1 = s0 + min(p.zseg, p.nz - z0);
+        s0 = col * nzr + z0;
+        s1 = s0 + min(p.zseg, nzr - z0);
     } else {
-        const long long W = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV) * p.nz;
+        const long long W = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV) * nzr;
         const long long share = (W + gridDim.x - 1) / gridDim.x;
         s0 = (long long)blockIdx.x * share;
         s1 = min(W, s0 + share);
     }
-    run_share<TYV>(p.nx, p.ny, p.nz, s0, s1,
+    run_share<TYV>(p.nx, nzr, p.zlo, s0, s1,
                    [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV, REP, OBS>(p, bx, by, z0, z1); });
 }
 
@@ -894,7 +907,7 @@ __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>())
     const int4 w = work[blockIdx.x];
     if (threadIdx.x == 0) sp = boxes[w.x];
     __syncthreads();
-    run_share<TYV>(sp.nx, sp.ny, sp.nz, w.y, w.z,
+    run_share<TYV>(sp.nx, sp.nz, 0, w.y, w.z,
                    [&](int bx, int by, int z0, int z1) { step_body<LAT, HO, TC, S, R, TYV, REP, OBS>(sp, bx, by, z0, z1); });
 }
 

@@ -111,15 +111,19 @@ __device__ void node_state(const BoundaryArgs& a, int x, int y, int z, long long
     const long long plane = (long long)a.nx * a.ny, N = plane * a.nz;
     const S* min = static_cast<const S*>(a.min);
     const double cssq = 1.0 / 3.0;
-    double P;
-    if constexpr (CD::scaled) P = a.pres_in[g];
-    else P = (double)CD::ld(min, g, 1.0);
-    double u = (double)CD::ld(min + N, g, 1.0 / a.scale[1]);
-    double v = (double)CD::ld(min + 2 * N, g, 1.0 / a.scale[2]);
-    double w = (double)CD::ld(min + 3 * N, g, 1.0 / a.scale[3]);
+    using LY = Layout<S>;
+    double P, u, v, w;
+    if constexpr (LY::split) {
+        P = a.pres_in[g]; u = a.pres_in[N + g]; v = a.pres_in[2 * N + g]; w = a.pres_in[3 * N + g];
+    } else {
+        P = (double)CD::ld(min, g, 1.0);
+        u = (double)CD::ld(min + N, g, 1.0 / a.scale[1]);
+        v = (double)CD::ld(min + 2 * N, g, 1.0 / a.scale[2]);
+        w = (double)CD::ld(min + 3 * N, g, 1.0 / a.scale[3]);
+    }
     double pi[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) pi[f] = (double)CD::ld(min + (4 + f) * N, g, 1.0 / a.scale[4 + f]);
+    for (int f = 0; f < 6; ++f) pi[f] = (double)CD::ld(min + LY::off(4 + f, N), g, 1.0 / a.scale[4 + f]);
     if constexpr (CD::scaled) {  // 16-bit storage keeps Pi - u u
         pi[0] += u * u; pi[1] += v * v; pi[2] += w * w;
         pi[3] += u * v; pi[4] += u * w; pi[5] += v * w;
@@ -254,11 +258,17 @@ __device__ void node_state(const BoundaryArgs& a, int x, int y, int z, long long
 // (Pi = sum f (c c - cs^2 delta)), and back
 template <typename S> __device__ void load_out(const BoundaryArgs& a, long long g, long long N, double (&o)[10]) {
     using CD = Codec<S>;
+    using LY = Layout<S>;
     const S* mom = static_cast<const S*>(a.mom);
-    if constexpr (CD::scaled) o[0] = a.pres[g];
-    else o[0] = (double)CD::ld(mom, g, 1.0);
+    if constexpr (LY::split) {
 #pragma unroll
-    for (int f = 1; f < 10; ++f) o[f] = (double)CD::ld(mom + f * N, g, 1.0 / a.scale[f]);
+        for (int f = 0; f < 4; ++f) o[f] = a.pres[f * N + g];
+    } else {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) o[f] = (double)CD::ld(mom + f * N, g, 1.0 / a.scale[f]);
+    }
+#pragma unroll
+    for (int f = 4; f < 10; ++f) o[f] = (double)CD::ld(mom + LY::off(f, N), g, 1.0 / a.scale[f]);
     if constexpr (CD::scaled) {  // 16-bit storage keeps Pi - u u
         o[4] += o[1] * o[1]; o[5] += o[2] * o[2]; o[6] += o[3] * o[3];
         o[7] += o[1] * o[2]; o[8] += o[1] * o[3]; o[9] += o[2] * o[3];
@@ -267,16 +277,19 @@ template <typename S> __device__ void load_out(const BoundaryArgs& a, long long 
 template <typename S> __device__ void store_out(const BoundaryArgs& a, long long g, long long N, double (&o)[10]) {
     using R = typename std::conditional<sizeof(S) == 8, double, float>::type;
     using CD = Codec<S>;
+    using LY = Layout<S>;
     S* mom = static_cast<S*>(a.mom);
-    if constexpr (CD::scaled) {
-        a.pres[g] = (float)o[0];
+    if constexpr (LY::split) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) a.pres[f * N + g] = (float)o[f];
         o[4] -= o[1] * o[1]; o[5] -= o[2] * o[2]; o[6] -= o[3] * o[3];
         o[7] -= o[1] * o[2]; o[8] -= o[1] * o[3]; o[9] -= o[2] * o[3];
     } else {
-        CD::st(mom, g, (R)o[0], R(1));
+#pragma unroll
+        for (int f = 0; f < 4; ++f) CD::st(mom + f * N, g, (R)o[f], (R)a.scale[f]);
     }
 #pragma unroll
-    for (int f = 1; f < 10; ++f) CD::st(mom + f * N, g, (R)o[f], (R)a.scale[f]);
+    for (int f = 4; f < 10; ++f) CD::st(mom + LY::off(f, N), g, (R)o[f], (R)a.scale[f]);
 }
 
 // add fp times the moment weights of link (dx, dy, dz) (reference convention)
@@ -430,8 +443,8 @@ __global__ void bounce_back_kernel(const BoundaryArgs a) {
 }
 
 template <typename S>
-__global__ void phi_flux_kernel(int nx, int ny, int nz, int axis, int side, const S* mom, const void* phi_,
-                                const int8_t* isf, double inv_scale, double* out) {
+__global__ void phi_flux_kernel(int nx, int ny, int nz, int axis, int side, const S* mom, const float* pres,
+                                const void* phi_, const int8_t* isf, double inv_scale, double* out) {
     using SP = typename PhiStore<S>::type;
     using CD = Codec<S>;
     const SP* phi = static_cast<const SP*>(phi_);
@@ -439,7 +452,9 @@ __global__ void phi_flux_kernel(int nx, int ny, int nz, int axis, int side, cons
     const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
     const long long tot = (long long)n[a1] * n[a2];
     const long long plane = (long long)nx * ny, N = plane * nz;
+    // the velocity component normal to the face (FP32 with 16-bit storage)
     const S* un = mom + (1 + axis) * N;
+    const float* un32 = Layout<S>::split ? pres + (1 + axis) * N : nullptr;
     double acc = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
          t += (long long)gridDim.x * blockDim.x) {
@@ -449,7 +464,7 @@ __global__ void phi_flux_kernel(int nx, int ny, int nz, int axis, int side, cons
         x[a2] = (int)(t / n[a1]);
         const long long g = x[2] * plane + (long long)x[1] * nx + x[0];
         if (isf[g] != -1) continue;
-        const double q = (double)CD::ld(un, g, inv_scale) * (double)phi[g];
+        const double q = (un32 ? (double)un32[g] : (double)CD::ld(un, g, inv_scale)) * (double)phi[g];
         acc += side ? -q : q;
     }
     __shared__ double red[256];
@@ -492,8 +507,9 @@ cudaError_t launch_bounce_back(int storage, const BoundaryArgs& a, cudaStream_t 
     });
 }
 
-cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const void* phi,
-                            const int8_t* isf, const double* inv_scale, double* d_flux, cudaStream_t st) {
+cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const void* mom, const float* pres,
+                            const void* phi, const int8_t* isf, const double* inv_scale, double* d_flux,
+                            cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(d_flux, 0, sizeof(double), st);
     if (e != cudaSuccess) return e;
     const int n[3] = {nx, ny, nz};
@@ -504,7 +520,7 @@ cudaError_t launch_phi_flux(int storage, int nx, int ny, int nz, int open, const
             const long long tot = (long long)n[axis == 0 ? 1 : 0] * n[axis == 2 ? 1 : 2];
             for (int side = 0; side < 2; ++side)
                 phi_flux_kernel<S><<<grid_for(tot, 256), 256, 0, st>>>(nx, ny, nz, axis, side,
-                                                                       static_cast<const S*>(mom), phi, isf,
+                                                                       static_cast<const S*>(mom), pres, phi, isf,
                                                                        inv_scale[1 + axis], d_flux);
         }
         return cudaGetLastError();

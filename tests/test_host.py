@@ -233,3 +233,40 @@ def test_vtk_files_in_the_reference_layout(tmp_path):
         assert np.array_equal(np.frombuffer(b[439:439 + n], np.float32), data.reshape(-1))
         assert b[439 + n:] == b"\n  </AppendedData>\n</VTKFile>\n"
     assert not (tmp_path / "out_press_000012.vti").exists()
+
+
+def test_printhalf_files_in_the_reference_layout(tmp_path):
+    """PRINTHALF (vars_module.f90:184-188, print_module.f90:110-121 and
+    2053-2164): the print values rounded to IEEE binary16, written as their
+    bit patterns; the VTK DataArray says UnsignedShort (a 121-byte header
+    line, so a 441-byte header), the XDMF NumberType="UInt" Precision="2".
+    Values include subnormals, overflow and exact halfway cases, which must
+    round to nearest even as numpy's float16 does."""
+    lx, ly, lz = 12, 5, 3
+    rng = np.random.default_rng(9)
+    rho = rng.standard_normal((lz, ly, lx)).astype(np.float32)
+    special = np.array([0.0, -0.0, 1e-8, 3e-5, 6.1e-5, 65504.0, 65520.0, 1e6, -1e6, 1.0 + 2.0 ** -11,
+                        1.0 + 3 * 2.0 ** -11, 2.0 ** -24, 2.0 ** -25, 1.5 * 2.0 ** -25, np.inf, -np.inf],
+                       dtype=np.float32)
+    rho.reshape(-1)[:special.size] = special
+    vel = rng.standard_normal((3, lz, ly, lx)).astype(np.float32) * 1e-3
+    L.write_vtk(str(tmp_path), 3, rho, vel, half=True)
+    b = (tmp_path / "out_rho_000003.vti").read_bytes()
+    line = (f'        <DataArray type="UnsignedShort" Name="{"rho":<8s}" NumberOfComponents="1" '
+            f'format="appended" offset="{0:>12d}"/>')
+    assert len(line) == 120
+    assert b[:441].decode().endswith('  <AppendedData encoding="raw">\n_')
+    assert line.encode() in b[:441]
+    n = lx * ly * lz * 2
+    assert np.frombuffer(b[441:445], np.int32)[0] == n
+    with np.errstate(over="ignore"):  # 1e6 overflows to infinity, as intended
+        want = rho.reshape(-1).astype(np.float16).view(np.uint16)
+    assert np.array_equal(np.frombuffer(b[445:445 + n], np.uint16), want)
+    assert len(b) == 445 + n + 30
+    L.write_raw_xdmf(str(tmp_path), 4, rho, vel, half=True)
+    r = np.fromfile(tmp_path / "out_rho_000004.raw", dtype=np.uint16)
+    assert np.array_equal(r, want)
+    v = np.fromfile(tmp_path / "out_vel_000004.raw", dtype=np.uint16).reshape(lz, ly, lx, 3)
+    assert np.array_equal(v, np.moveaxis(vel, 0, -1).astype(np.float16).view(np.uint16))
+    x = (tmp_path / "out_vel_000004.xdmf").read_text()
+    assert 'NumberType="UInt" Precision="2" Dimensions="3 5 12 3"' in x
