@@ -59,6 +59,9 @@ B_LUP = {"f32": 112, "f16": 64, "bf16": 64, "f64": 224}  # algorithmic bytes per
 # DRAM bytes (read + write) of one step launch of the tuned kernel, measured
 # by ncu (dram__bytes_read.sum + dram__bytes_write.sum) at this workload
 NCU_TRAFFIC = {("f32", 256): 1854044160}
+# warp instructions of one step launch (ncu smsp__inst_executed.sum) at this
+# workload: the issue ceiling is 4 warp instructions per SM cycle
+NCU_WARP_INST = {("f32", 256): 723.6e6}
 
 
 CHANNEL = (512, 256, 256)  # the two-component channel with obstacles (lx, ly, lz)
@@ -678,6 +681,19 @@ def main():
         shutdown(world)
         return
     traffic = NCU_TRAFFIC.get((args.storage, args.box)) if args.workload == "laplace" else None
+    winst = NCU_WARP_INST.get((args.storage, args.box)) if args.workload == "laplace" else None
+    issue = None
+    if winst:
+        # the instruction-issue ceiling of the step: every SM issuing one warp
+        # instruction per scheduler (4) per cycle at the sampled SM clock
+        import torch
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = r["clocks"].get("sm_mhz") or 1965.0
+        n = args.box ** 3
+        ceiling = nsm * 4 * mhz * 1e6 / (winst / n) / 1e6
+        issue = {"warp_inst_per_launch": winst, "thread_inst_per_node": winst * 32 / n, "sms": nsm, "sm_mhz": mhz,
+                 "ceiling_mlups": ceiling, "frac": r["value"] / world / ceiling,
+                 "source": "ncu smsp__inst_executed.sum of one step launch (profiles/)"}
     nbox = box_of(args.workload, args.box)
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -687,7 +703,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": peak, "unit": "GB/s",
                      "frac": r["achieved"] / peak, "traffic": traffic, "peak_source": peak_src,
                      "kernel": "lbf::stream_kernel<27,HO,TC>", "launch": r["tuning"],
-                     "bytes_per_launch": bytes_per_lup(args.storage, args.workload) * nbox[0] * nbox[1] * nbox[2]},
+                     "bytes_per_launch": bytes_per_lup(args.storage, args.workload) * nbox[0] * nbox[1] * nbox[2],
+                     "issue": issue},
         "e2e": r["e2e"], "gpu_launches": args.steps * (2 if args.workload == "channel" else 1), "clocks": r["clocks"],
         "cpu_baseline": cpu,
         "finite": r["finite"], "extra": extra, "serving": serving,
