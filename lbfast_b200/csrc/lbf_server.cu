@@ -114,6 +114,9 @@ int solve_tile(const lbf_params& p) { return p.tile_y ? p.tile_y : 8; }
 struct lbf_server {
     lbf_server_config cfg{};
     cudaStream_t stream = nullptr;
+    // uploads and set-up of newly admitted solves, which overlap the chunk of
+    // steps running on `stream`
+    cudaStream_t upload = nullptr;
     long long next_id = 1;
     std::map<long long, std::unique_ptr<Solve>> solves;
     std::deque<Solve*> queue;
@@ -162,11 +165,15 @@ int admit(lbf_server* s) {
         s->queue.pop_front();
         lbf_handle* h = nullptr;
         int rc = lbf_create(&v->p, &h);
-        if (rc == LBF_OK) rc = lbf_set_stream(h, s->stream);
+        if (rc == LBF_OK) rc = lbf_set_stream(h, s->upload);
         if (rc == LBF_OK && v->p.obstacles) rc = lbf_set_isfluid(h, v->isf.data());
         if (rc == LBF_OK)
             rc = lbf_set_fields(h, v->mom.data(), v->p.twocomponent ? v->phi.data() : nullptr, v->dtype);
         if (rc == LBF_OK) rc = lbf::handle_prime(h);
+        // the solve's state is complete before it joins the steps on `stream`
+        if (rc == LBF_OK && cudaStreamSynchronize(s->upload) != cudaSuccess)
+            rc = sfail(LBF_E_CUDA, "solve set-up failed");
+        if (rc == LBF_OK) rc = lbf_set_stream(h, s->stream);
         if (rc != LBF_OK) {
             char msg[512];
             lbf_last_error(msg, sizeof msg);
@@ -401,7 +408,9 @@ int lbf_server_create(const lbf_server_config* cfg, lbf_server** out) {
         s->cfg.mem_budget = (long long)(0.8 * (double)fr);
     }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        if (s->stream) cudaStreamDestroy(s->stream);
         delete s;
         return sfail(LBF_E_CUDA, "stream: %s", cudaGetErrorString(e));
     }
@@ -416,6 +425,7 @@ int lbf_server_destroy(lbf_server* s) {
     for (Solve* v : s->active) release(s, v);
     for (auto& kv : s->batches) free_batch(kv.second);
     cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->upload);
     delete s;
     return LBF_OK;
 }
@@ -456,7 +466,7 @@ int lbf_server_run(lbf_server* s, int max_chunks, int* active, int* queued) {
     if (!s) return sfail(LBF_E_ARG, "lbf_server_run: null server");
     int rc = LBF_OK;
     for (int c = 0; c < max_chunks && rc == LBF_OK; ++c) {
-        admit(s);
+        if (c == 0) admit(s);
         if (s->active.empty()) break;
         if (s->dirty && (rc = rebuild(s))) break;
         long long L = s->cfg.chunk;
@@ -474,6 +484,9 @@ int lbf_server_run(lbf_server* s, int max_chunks, int* active, int* queued) {
             if (rc) break;
             for (Solve* v : s->active) v->done += L;
         }
+        // solves that fit next to the resident ones are uploaded while the
+        // chunk runs; they join at the next rebuild
+        admit(s);
         cudaError_t e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) {
             rc = sfail(LBF_E_CUDA, "server step: %s", cudaGetErrorString(e));

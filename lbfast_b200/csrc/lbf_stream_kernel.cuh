@@ -125,11 +125,24 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     {
         const int r = t - NTH;
         if (r >= 0 && r < NRING1) {
-            if (r < R1X) nodeB = r;                                        // top row
-            else if (r < 2 * R1X) nodeB = (R1Y - 1) * R1X + (r - R1X);     // bottom row
-            else if (r < 2 * R1X + TY) nodeB = (r - 2 * R1X + 1) * R1X;    // left column
-            else nodeB = (r - 2 * R1X - TY + 1) * R1X + (R1X - 1);         // right column
+            // one kind of ring node per warp: the inner 32 nodes of the top row,
+            // of the bottom row, then the left and right columns with the corners
+            if (r < TX) nodeB = r + 1;                                              // top row
+            else if (r < 2 * TX) nodeB = (R1Y - 1) * R1X + (r - TX + 1);            // bottom row
+            else if (r < 2 * TX + R1Y) nodeB = (r - 2 * TX) * R1X;                  // left column
+            else nodeB = (r - 2 * TX - R1Y) * R1X + (R1X - 1);                      // right column
         }
+    }
+    // ring nodes stream into the tile along one axis only: the rows' along y
+    // (cy = +1 from the top row, -1 from the bottom), the columns' along x
+    // (cx = +1 from the left, -1 from the right; corners with them).  ring_col
+    // is uniform across a warp (the ring warps hold 32 row nodes each, then
+    // the columns).
+    const bool ring_col = (t - NTH) >= 2 * TX;
+    R ring_dir = R(0);
+    if (nodeB >= 0) {
+        const int bx = nodeB % R1X, by = nodeB / R1X;
+        ring_dir = ring_col ? (bx == 0 ? R(1) : R(-1)) : (by == 0 ? R(1) : R(-1));
     }
     // wrapped: the node was reached across a periodic face in x or y
     auto r1_geom = [&](int node, int& off, bool& wrapped) -> bool {
@@ -470,6 +483,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             const bool live = inb && (isf != 0);
             const bool interior = (k == 0) && out_ok && q_inner;
             R fpop[27];
+            bool ring_done = false;  // a ring node's populations are stored already
             R sP = 0, spxx = 0, spyy = 0, spzz = 0, spxy = 0, spxz = 0, spyz = 0, som = 0;
             if (live) {
                 R P, u, v, w, pxx, pyy, pzz, pxy, pxz, pyz;
@@ -703,25 +717,75 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                         M[2][2][0] = M[2][0][2] = M[0][2][2] = M[1][1][2] = M[1][2][1] = M[2][1][1] = R(0);
                         M[2][1][2] = M[2][2][1] = M[1][2][2] = M[2][2][2] = R(0);
                     }
-                    R T[3][3][3];
+                    if (k == 1 && ring_col) {
+                        // column ring node: the x transform at cx = ring_dir only,
+                        // the same operations as the full transform for that value
+                        R T[3][3];  // [b][c]
 #pragma unroll
-                    for (int b = 0; b < 3; ++b)
+                        for (int b = 0; b < 3; ++b)
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) d1q3_inv<R>(M[0][b][c], M[1][b][c], M[2][b][c], T[0][b][c], T[1][b][c], T[2][b][c]);
+                            for (int c = 0; c < 3; ++c) {
+                                const R sv = fmaf_t(M[0][b][c], R(1.0 / 6.0), R(0.5) * M[2][b][c]);
+                                T[b][c] = sv + ring_dir * (R(0.5) * M[1][b][c]);
+                            }
+                        R Y[3][3];  // [b][c]
 #pragma unroll
-                    for (int a = 0; a < 3; ++a)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) d1q3_inv<R>(T[a][0][c], T[a][1][c], T[a][2][c], M[a][0][c], M[a][1][c], M[a][2][c]);
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
+                        for (int c = 0; c < 3; ++c) d1q3_inv<R>(T[0][c], T[1][c], T[2][c], Y[0][c], Y[1][c], Y[2][c]);
+                        const int xg = ring_dir > R(0) ? 2 : 0;
 #pragma unroll
                         for (int b = 0; b < 3; ++b) {
                             R vm, v0, vp;
-                            d1q3_inv<R>(M[a][b][0], M[a][b][1], M[a][b][2], vm, v0, vp);
-                            fpop[LINK(a - 1, b - 1, -1)] = vm;
-                            fpop[LINK(a - 1, b - 1, 0)] = v0;
-                            fpop[LINK(a - 1, b - 1, 1)] = vp;
+                            d1q3_inv<R>(Y[b][0], Y[b][1], Y[b][2], vm, v0, vp);
+                            R2 v2;
+                            v2.x = vm;
+                            v2.y = v0;
+                            pops2[(3 * b + xg) * R1N + node] = v2;
+                            pops1[(3 * b + xg) * R1N + node] = vp;
                         }
+                        ring_done = true;
+                    } else {
+                        R T[3][3][3];
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) d1q3_inv<R>(M[0][b][c], M[1][b][c], M[2][b][c], T[0][b][c], T[1][b][c], T[2][b][c]);
+                        if (k == 1) {
+                            // row ring node: the y transform at cy = ring_dir only
+                            const int yg = ring_dir > R(0) ? 2 : 0;
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                R Y[3];
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    const R sv = fmaf_t(T[a][0][c], R(1.0 / 6.0), R(0.5) * T[a][2][c]);
+                                    Y[c] = sv + ring_dir * (R(0.5) * T[a][1][c]);
+                                }
+                                R vm, v0, vp;
+                                d1q3_inv<R>(Y[0], Y[1], Y[2], vm, v0, vp);
+                                R2 v2;
+                                v2.x = vm;
+                                v2.y = v0;
+                                pops2[(3 * yg + a) * R1N + node] = v2;
+                                pops1[(3 * yg + a) * R1N + node] = vp;
+                            }
+                            ring_done = true;
+                        } else {
+#pragma unroll
+                            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) d1q3_inv<R>(T[a][0][c], T[a][1][c], T[a][2][c], M[a][0][c], M[a][1][c], M[a][2][c]);
+#pragma unroll
+                            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                                for (int b = 0; b < 3; ++b) {
+                                    R vm, v0, vp;
+                                    d1q3_inv<R>(M[a][b][0], M[a][b][1], M[a][b][2], vm, v0, vp);
+                                    fpop[LINK(a - 1, b - 1, -1)] = vm;
+                                    fpop[LINK(a - 1, b - 1, 0)] = v0;
+                                    fpop[LINK(a - 1, b - 1, 1)] = vp;
+                                }
+                        }
+                    }
                 } else {
                     // D3Q19 / D3Q15: the second-order expansion link by link (D3Q27 indices)
                     const R base = m0 - R(1.5) * (mxx + myy + mzz);
@@ -742,6 +806,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             }
 #pragma unroll
             for (int g = 0; g < 9; ++g) {
+                if (ring_done) break;
                 const int cx = g % 3 - 1, cy = g / 3 - 1;
                 // links the lattice lacks carry 0 (D3Q19: no corners, D3Q15: no edges)
                 R2 v;
