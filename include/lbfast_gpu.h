@@ -201,6 +201,14 @@ int lbf_create_slab(const lbf_params* global, int z0, int z1, lbf_handle** h);
 int lbf_slab_nregions(lbf_handle* h, int* n);
 int lbf_slab_region(lbf_handle* h, int side, int recv, int field, void** ptr, size_t* bytes);
 int lbf_slabs_exchange(lbf_handle* const* slabs, int n);
+/* nsteps steps of the slabs of one process (on one GPU or several) with the
+ * halo exchange of each step overlapped with the planes that do not read the
+ * halos (4 planes from each face inward), as the reference's ASYNCMPI split
+ * does (integrator_module.f90:278-368): per slab the inner planes run while
+ * the halos of the step's input are copied on a second stream, then the
+ * planes next to the halos.  Primes fresh slabs and exchanges once first;
+ * ends with the halos of the new time level filled. */
+int lbf_slabs_step(lbf_handle* const* slabs, int n, int nsteps);
 
 /* ---- full-state checkpoint ----
  * No counterpart in the reference, whose restart (lbf_write_restart_raw) is

@@ -30,7 +30,7 @@ EXPORTED = (
     "lbf_server_poll", "lbf_server_fetch", "lbf_server_cancel", "lbf_get_tuning", "lbf_write_restart_raw",
     "lbf_read_restart_raw", "lbf_write_vtk", "lbf_write_vtk_half", "lbf_write_raw_xdmf_half",
     "lbf_write_checkpoint", "lbf_read_checkpoint", "lbf_create_slab", "lbf_slab_nregions", "lbf_slab_region",
-    "lbf_slabs_exchange",
+    "lbf_slabs_exchange", "lbf_slabs_step",
 )
 SOLVE_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -99,6 +99,7 @@ def load() -> C.CDLL:
     lib.lbf_slab_nregions.argtypes = [vp, P(C.c_int)]
     lib.lbf_slab_region.argtypes = [vp, C.c_int, C.c_int, C.c_int, P(vp), P(C.c_size_t)]
     lib.lbf_slabs_exchange.argtypes = [P(vp), C.c_int]
+    lib.lbf_slabs_step.argtypes = [P(vp), C.c_int, C.c_int]
     lib.lbf_write_checkpoint.argtypes = [vp, C.c_char_p]
     lib.lbf_read_checkpoint.argtypes = [vp, C.c_char_p]
     lib.lbf_mark_isfluid.argtypes = [C.c_int] * 8 + [i8p, i8p]

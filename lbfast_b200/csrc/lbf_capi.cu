@@ -93,6 +93,9 @@ void free_all(lbf_handle* h) {
     cudaFree(h->d_rnrm);
     cudaFree(h->d_rep);
     cudaFree(h->staging);
+    if (h->xstream) cudaStreamDestroy(h->xstream);
+    if (h->ev_done) cudaEventDestroy(h->ev_done);
+    if (h->ev_copied) cudaEventDestroy(h->ev_copied);
 }
 
 // automatic z segment: enough CTAs for about four waves on 148 SMs (two CTAs
@@ -869,6 +872,41 @@ bool slab_field(lbf_handle* h, int f, char** base, size_t* plane_bytes) {
 int slab_nfields(const lbf_handle* h) { return 13 + (h->tc ? 1 : 0); }
 }  // namespace
 
+extern "C" int lbf_slab_region(lbf_handle* h, int side, int recv, int field, void** ptr, size_t* bytes);
+
+namespace {
+// check that the slabs form one box's ring and can be exchanged
+int check_slabs(lbf_handle* const* slabs, int n, const char* who) {
+    if (!slabs || n < 1) return fail(LBF_E_ARG, "%s: no slabs", who);
+    for (int i = 0; i < n; ++i) {
+        if (!slabs[i] || !slabs[i]->slab) return fail(LBF_E_ARG, "%s: handle %d is not a slab", who, i);
+        if (slab_nfields(slabs[i]) != slab_nfields(slabs[0]) || slabs[i]->storage != slabs[0]->storage ||
+            slabs[i]->nx != slabs[0]->nx || slabs[i]->ny != slabs[0]->ny)
+            return fail(LBF_E_ARG, "%s: slab %d does not match slab 0", who, i);
+        if (!slabs[i]->fields_set) return fail(LBF_E_STATE, "%s: slab %d has no fields", who, i);
+    }
+    return LBF_OK;
+}
+
+// copy the halo regions of slab i's current time level from its neighbours, on stream st
+int slab_recv(lbf_handle* const* slabs, int n, int i, cudaStream_t st) {
+    lbf_handle* lo = slabs[(i + n - 1) % n];
+    lbf_handle* hi = slabs[(i + 1) % n];
+    for (int f = 0; f < slab_nfields(slabs[i]); ++f) {
+        void *dst, *src;
+        size_t b, b2;
+        lbf_slab_region(slabs[i], 0, 1, f, &dst, &b);
+        lbf_slab_region(lo, 1, 0, f, &src, &b2);
+        CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, st));
+        lbf_slab_region(slabs[i], 1, 1, f, &dst, &b);
+        lbf_slab_region(hi, 0, 0, f, &src, &b2);
+        CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, st));
+    }
+    return LBF_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int lbf_create_slab(const lbf_params* global, int z0, int z1, lbf_handle** out) {
@@ -891,6 +929,7 @@ int lbf_create_slab(const lbf_params* global, int z0, int z1, lbf_handle** out) 
     h->zg0 = z0;
     h->nzs = z1 - z0;
     h->nzg = global->lz;
+    cudaGetDevice(&h->device);
     return LBF_OK;
 }
 
@@ -928,23 +967,94 @@ int lbf_slabs_exchange(lbf_handle* const* slabs, int n) {
     }
     // every slab's step must be complete before its planes are copied
     for (int i = 0; i < n; ++i) CUDA_TRY(cudaStreamSynchronize(slabs[i]->stream));
-    const int nf = slab_nfields(slabs[0]);
     for (int i = 0; i < n; ++i) {
-        lbf_handle* lo = slabs[(i + n - 1) % n];  // the slab below (periodic ring)
-        lbf_handle* hi = slabs[(i + 1) % n];      // the slab above
-        for (int f = 0; f < nf; ++f) {
-            void *dst, *src;
-            size_t b, b2;
-            lbf_slab_region(slabs[i], 0, 1, f, &dst, &b);
-            lbf_slab_region(lo, 1, 0, f, &src, &b2);
-            CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, slabs[i]->stream));
-            lbf_slab_region(slabs[i], 1, 1, f, &dst, &b);
-            lbf_slab_region(hi, 0, 0, f, &src, &b2);
-            CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, slabs[i]->stream));
-        }
+        int rc = slab_recv(slabs, n, i, slabs[i]->stream);
+        if (rc) return rc;
     }
     for (int i = 0; i < n; ++i) CUDA_TRY(cudaStreamSynchronize(slabs[i]->stream));
     return LBF_OK;
+}
+
+int lbf_slabs_step(lbf_handle* const* slabs, int n, int nsteps) {
+    int rc = check_slabs(slabs, n, "lbf_slabs_step");
+    if (rc) return rc;
+    if (nsteps < 0) return fail(LBF_E_ARG, "lbf_slabs_step: nsteps < 0");
+    int dev0 = 0;
+    CUDA_TRY(cudaGetDevice(&dev0));
+    // the pre-loop wetting of every slab, then the halos of the first input
+    bool fresh = false;
+    for (int i = 0; i < n && !rc; ++i) {
+        lbf_handle* h = slabs[i];
+        CUDA_TRY(cudaSetDevice(h->device));
+        if (!h->primed) {
+            rc = prime(h);
+            fresh = true;
+        }
+        if (!rc && !h->tuned && nsteps > 0) rc = autotune(h);
+        if (!rc && !h->xstream) {
+            cudaError_t e = cudaStreamCreateWithFlags(&h->xstream, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_copied, cudaEventDisableTiming);
+            if (e != cudaSuccess) rc = fail(LBF_E_CUDA, "lbf_slabs_step: %s", cudaGetErrorString(e));
+        }
+    }
+    if (!rc && fresh) rc = lbf_slabs_exchange(slabs, n);
+    const int H = lbf::SLAB_HALO;
+    for (int s = 0; s < nsteps && !rc; ++s) {
+        // every slab's previous step is done before its planes are sent
+        for (int i = 0; i < n && !rc; ++i) {
+            cudaSetDevice(slabs[i]->device);
+            if (cudaEventRecord(slabs[i]->ev_done, slabs[i]->stream) != cudaSuccess)
+                rc = fail(LBF_E_CUDA, "lbf_slabs_step: event record failed");
+        }
+        for (int i = 0; i < n && !rc; ++i) {
+            lbf_handle* h = slabs[i];
+            cudaSetDevice(h->device);
+            const bool write_u = h->dr || s == nsteps - 1;
+            lbf::StepArgs a;
+            lbf::handle_step_args(h, a, write_u);
+            // the planes whose stencils stay clear of the halos (4 planes
+            // from each face: phi of the collision's theta neighbours) run
+            // while the halos of this step's input arrive
+            const int in_lo = H + 4, in_hi = H + h->nzs - 4;
+            if (in_hi > in_lo) {
+                a.zlo = in_lo;
+                a.zhi = in_hi;
+                cudaError_t e = h->launcher(a, h->stream);
+                if (e != cudaSuccess) { rc = fail(LBF_E_CUDA, "slab step: %s", cudaGetErrorString(e)); break; }
+            }
+            for (int j : {(i + n - 1) % n, (i + 1) % n, i})
+                if (cudaStreamWaitEvent(h->xstream, slabs[j]->ev_done, 0) != cudaSuccess)
+                    rc = fail(LBF_E_CUDA, "lbf_slabs_step: stream wait failed");
+            if (!rc) rc = slab_recv(slabs, n, i, h->xstream);
+            if (!rc && cudaEventRecord(h->ev_copied, h->xstream) != cudaSuccess)
+                rc = fail(LBF_E_CUDA, "lbf_slabs_step: event record failed");
+            if (!rc && cudaStreamWaitEvent(h->stream, h->ev_copied, 0) != cudaSuccess)
+                rc = fail(LBF_E_CUDA, "lbf_slabs_step: stream wait failed");
+            // the per-step work that reads the halos (wetting), then the planes next to them
+            if (!rc) rc = lbf::handle_pre_step(h);
+            if (rc) break;
+            const int ranges[2][2] = {{H, in_hi > in_lo ? in_lo : H + h->nzs}, {in_hi > in_lo ? in_hi : H + h->nzs, H + h->nzs}};
+            for (const auto& r : ranges) {
+                if (r[1] <= r[0]) continue;
+                a.zlo = r[0];
+                a.zhi = r[1];
+                cudaError_t e = h->launcher(a, h->stream);
+                if (e != cudaSuccess) { rc = fail(LBF_E_CUDA, "slab step: %s", cudaGetErrorString(e)); break; }
+            }
+        }
+        // all slabs advance together: a slab's next send reads the planes this step wrote
+        for (int i = 0; i < n && !rc; ++i) {
+            lbf_handle* h = slabs[i];
+            cudaSetDevice(h->device);
+            lbf::handle_advance(h, h->dr || s == nsteps - 1);
+            rc = lbf::handle_post_step(h);
+        }
+    }
+    // the halos of the new time level, for lbf_get_fields and the next call
+    if (!rc) rc = lbf_slabs_exchange(slabs, n);
+    cudaSetDevice(dev0);
+    return rc;
 }
 
 }  // extern "C"

@@ -57,6 +57,11 @@ struct lbf_handle {
     // neighbouring slabs; zg0 is the slab's first plane in the global box of nzg
     bool slab = false;
     int zg0 = 0, nzs = 0, nzg = 0;
+    // overlapped slab steps (lbf_slabs_step): the device, a stream for the
+    // halo copies and events marking a step's end and the copies' end
+    int device = 0;
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t ev_done = nullptr, ev_copied = nullptr;
 };
 
 namespace lbf {

@@ -149,7 +149,14 @@ class SlabSet:
     def exchange(self) -> None:
         check(load().lbf_slabs_exchange(self._arr, len(self.slabs)))
 
-    def step(self, n: int = 1) -> None:
+    def step(self, n: int = 1, overlap: bool = True) -> None:
+        """n steps.  overlap: lbf_slabs_step, each step's halo copies running
+        beside the planes that do not read them; else one lbf_step per slab
+        and a full exchange after it."""
+        if overlap:
+            check(load().lbf_slabs_step(self._arr, len(self.slabs), int(n)))
+            self.primed = True
+            return
         if not self.primed:
             # the pre-loop wetting runs in each slab's own planes; the halos
             # then take the neighbours' wetted planes

@@ -56,6 +56,7 @@ def test_fullsize_fp32_against_fp64(runs):
     fl = np.abs(isf) == 1
     assert np.all(np.isfinite(out["f64"][0][:, fl])) and np.all(np.isfinite(out["f64"][1][fl]))
     eu, ep = rel_l2(out["f32"][0][1:4], out["f64"][0][1:4], fl), rel_l2(out["f32"][1], out["f64"][1], fl)
+    print(f"channel 512x256x256 FP32 vs FP64 after {NSTEPS} steps: u {eu:.2e} phi {ep:.2e}")
     assert eu < 1e-4 and ep < 1e-5, (eu, ep)
 
 
@@ -71,6 +72,7 @@ def test_fullsize_fp16_against_fp64(runs):
     eu = rel_l2(out["f16"][0][1:4], out["f64"][0][1:4], fl)
     eP = rel_l2(out["f16"][0][0:1], out["f64"][0][0:1], fl)
     ep = rel_l2(out["f16"][1], out["f64"][1], fl)
+    print(f"channel FP16 storage vs FP64 after {NSTEPS} steps: u {eu:.2e} P {eP:.2e} phi {ep:.2e}")
     assert eu < 1e-3 and eP < 1e-3 and ep < 1e-3, (eu, eP, ep)
 
 
@@ -83,4 +85,5 @@ def test_fullsize_bf16_against_fp64(runs):
     eu = rel_l2(out["bf16"][0][1:4], out["f64"][0][1:4], fl)
     eP = rel_l2(out["bf16"][0][0:1], out["f64"][0][0:1], fl)
     ep = rel_l2(out["bf16"][1], out["f64"][1], fl)
+    print(f"channel BF16 storage vs FP64 after {NSTEPS} steps: u {eu:.2e} P {eP:.2e} phi {ep:.2e}")
     assert eu < 1e-2 and eP < 1e-2 and ep < 1e-2, (eu, eP, ep)

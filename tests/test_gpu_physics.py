@@ -96,23 +96,29 @@ def test_taylor_green_viscous_decay_linear_regime():
 
 
 def test_taylor_green_config_matches_oracle():
-    """The reference's CPU case (64^3 D3Q19, nu = 0.01, u0 = 0.05): FP32 GPU
-    within 1e-5 rel-L2 of the FP64 oracle after 200 steps."""
+    """The reference's CPU case at its full length (64^3 D3Q19, nu = 0.01,
+    u0 = 0.05, 1000 steps): the FP32 GPU run within 1e-5 rel-L2 of the FP64
+    oracle after 200 and after 1000 steps, the FP64 GPU run within 1e-10."""
     n = 64
-    p = L.Params(lx=n, ly=n, lz=n, lattice=19, visc1=0.01)
-    m = L.ic_taylor_green(n, n, n, 0.05)
-    s = L.Solver(p)
-    s.set_fields(m)
-    s.step(200)
-    mg, _, _ = s.get_fields()
-    s.close()
     from oracle import oracle as O
-    o = O.Oracle(p.oracle_dict(), "f64")
-    o.set_isfluid(np.ones(p.shape, np.int8))
+    m = L.ic_taylor_green(n, n, n, 0.05)
+    o = O.Oracle(L.Params(lx=n, ly=n, lz=n, lattice=19, visc1=0.01).oracle_dict(), "f64")
+    o.set_isfluid(np.ones((n, n, n), np.int8))
     o.set_fields(m)
     o.step(200)
-    mo, _, _ = o.get_fields()
-    assert rel_l2(mg, mo) < 1e-5
+    ref = {200: o.get_fields()[0]}
+    o.step(800)
+    ref[1000] = o.get_fields()[0]
+    for storage, bar in (("f32", 1e-5), ("f64", 1e-10)):
+        s = L.Solver(L.Params(lx=n, ly=n, lz=n, lattice=19, visc1=0.01, storage=storage))
+        s.set_fields(m)
+        done = 0
+        for k in (200, 1000):
+            s.step(k - done)
+            done = k
+            err = rel_l2(s.get_fields()[0], ref[k])
+            assert err < bar, (storage, k, err)
+        s.close()
 
 
 def test_laplace_law():

@@ -15,8 +15,10 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("name,storage", [("q27ho_2c_dr", "f32"), ("q27ho_2c_dr", "f64"), ("obs_q27ho_2c_dr", "f32"),
                                           ("obs_q27ho_2c_dr_bb", "f32"), ("tg_q19", "f32"), ("q27_1c", "f32")])
-@pytest.mark.parametrize("nslabs", [1, 2, 3])
-def test_slabs_equal_the_single_box(name, storage, nslabs):
+@pytest.mark.parametrize("nslabs,overlap", [(1, True), (2, True), (3, True), (2, False)])
+def test_slabs_equal_the_single_box(name, storage, nslabs, overlap):
+    """overlap: lbf_slabs_step (the halo copies beside the inner planes);
+    else lbf_step per slab and a full exchange after each step."""
     p, isf, m, phi = make_case(name, storage)
     p.tile_y = 8 if storage == "f64" else 16
     a = L.Solver(p)
@@ -30,12 +32,13 @@ def test_slabs_equal_the_single_box(name, storage, nslabs):
     if p.obstacles:
         s.set_isfluid(isf)
     s.set_fields(m, phi)
-    s.step(12)
+    s.step(5, overlap=overlap)
+    s.step(7, overlap=overlap)
     got = s.get_fields()
     s.close()
     for x, y, what in zip(got, ref, ("moments", "phi", "u_old")):
         if y is not None:
-            assert np.array_equal(x, y, equal_nan=True), (name, storage, nslabs, what,
+            assert np.array_equal(x, y, equal_nan=True), (name, storage, nslabs, overlap, what,
                                                           float(np.nanmax(np.abs(x - y))))
 
 

@@ -86,6 +86,8 @@ def test_laplace256_fp32_against_fp64(laplace):
     ep = rel_l2(r["f32"][10000]["phi"], r["f64"][10000]["phi"])
     eP = rel_l2(r["f32"][10000]["P"], r["f64"][10000]["P"])
     eu = rel_l2(r["f32"][10000]["u"], r["f64"][10000]["u"])
+    print(f"laplace 256^3 FP32 vs FP64: 1000 steps phi {ep1:.2e} P {eP1:.2e}; 10000 steps phi {ep:.2e} P {eP:.2e} "
+          f"u {eu:.2e}")
     assert ep1 < 1e-5 and eP1 < 5e-5, (ep1, eP1)
     assert ep < 1e-4 and eP < 1e-3 and eu < 0.1, (ep, eP, eu)
 
@@ -116,6 +118,7 @@ def test_laplace256_fp16_against_fp64(laplace):
     for n in (1000, 10000):
         ep = rel_l2(r["f16"][n]["phi"], r["f64"][n]["phi"])
         eP = rel_l2(r["f16"][n]["P"], r["f64"][n]["P"])
+        print(f"laplace 256^3 FP16 storage vs FP64 after {n} steps: phi {ep:.2e} P {eP:.2e}")
         assert ep < 1e-3 and eP < 1e-3, (n, ep, eP)
 
 
@@ -134,4 +137,6 @@ def test_droplets768_fp32_and_fp16_against_fp64(droplets768):
     r = droplets768
     e32 = (rel_l2(r["f32"]["phi"], r["f64"]["phi"]), rel_l2(r["f32"]["u"], r["f64"]["u"]))
     e16 = (rel_l2(r["f16"]["phi"], r["f64"]["phi"]), rel_l2(r["f16"]["u"], r["f64"]["u"]))
+    print(f"768^3 droplets after 200 steps vs FP64: FP32 phi {e32[0]:.2e} u {e32[1]:.2e}; "
+          f"FP16 storage phi {e16[0]:.2e} u {e16[1]:.2e}")
     assert max(e32) < 1e-5 and max(e16) < 1e-3, (e32, e16)
