@@ -448,6 +448,9 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     prefetch_a(z0 - 1);
     cp_async_wait_all();
     __syncthreads();
+    // theta partials of the first loop plane; the loop computes each later
+    // plane's after the pull phase of the plane before
+    if constexpr (TC) theta_partials(z0);
 
     for (int q = z0 - 1; q <= z1; ++q) {
         bool zok = true;
@@ -457,12 +460,10 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 
         // ================= phase 1 =================
         // partials of phi(q+3), then theta(q+2) from the partials of planes
-        // q+1..q+3 (this thread's own nodes), and the theta partials of plane
-        // q+1 at this thread's collision nodes
+        // q+1..q+3 (this thread's own nodes)
         if constexpr (TC) {
             planar_plane(q + 3);
             theta_plane(q + 2);
-            theta_partials(q + 1);
         }
 
         // unrolled: the interior node's copy of the collision reads the
@@ -910,6 +911,12 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             a0[i] = ap[i];
             ap[i] = R(0);
         }
+        // the theta partials of plane q+2 at this thread's collision nodes
+        // (theta(q+2) is complete since the barrier after phase 1).  Here
+        // rather than in phase 1 they fill the shorter pull phase and shorten
+        // the collision phase, whose barrier waits for the ring collisions:
+        // 1.7 % per step at 256^3.
+        if constexpr (TC) theta_partials(q + 2);
         cp_async_wait_all();
         __syncthreads();
     }
