@@ -134,3 +134,34 @@ def mean_period(steps, series, min_dist: float):
     if len(peaks) < 2:
         return float("nan"), len(peaks)
     return float(np.mean(np.diff(peaks))), len(peaks)
+
+
+def first_extrema(steps, series, count: int = 3):
+    """The first `count` alternating extrema of `series` after its first
+    maximum, beginning with a minimum: [(t, value, kind)], each refined by the
+    parabola through the sampled extremum and its two neighbours.  A damped
+    oscillation's first cycle is measured this way before later small
+    wiggles, where counting every local maximum above the mean (mean_period,
+    the reference's method) picks up noise."""
+    s = np.asarray(series, dtype=np.float64)
+    t = np.asarray(steps, dtype=np.float64)
+    dt = t[1] - t[0]
+    out = []
+    # a series that falls from its first sample starts at its first maximum
+    want = "min" if s[0] >= s[1] else None
+    for i in range(1, len(s) - 1):
+        is_max = s[i] > s[i - 1] and s[i] >= s[i + 1]
+        is_min = s[i] < s[i - 1] and s[i] <= s[i + 1]
+        if want is None:
+            if is_max:
+                want = "min"
+            continue
+        if (want == "min" and is_min) or (want == "max" and is_max):
+            y0, y1, y2 = s[i - 1], s[i], s[i + 1]
+            den = y0 - 2.0 * y1 + y2
+            off = 0.5 * (y0 - y2) / den if den != 0 else 0.0
+            out.append((t[i] + off * dt, y1 - 0.25 * (y0 - y2) * off, want))
+            if len(out) == count:
+                break
+            want = "max" if want == "min" else "min"
+    return out

@@ -359,10 +359,17 @@ def test_lamb_oscillation_frequency():
     377-471, 959-1050; sigma 0.03, nu 0.001, equal densities of lamb.inp) of
     a droplet R = 20 in 128^3 with a small P2 surface perturbation
     (r = R (1 + 0.05 P2(cos theta)), where linear theory holds; the reference's
-    own LAMBTEST starts from a 2:1 ellipsoid, far outside it): the z half-axis
-    oscillates with a period 1.0-1.4 times Lamb's with the reference's viscous
-    correction; measured 1.26 times -- the scheme's, with a width-4 interface
-    on R = 20 (the FP64 step equals the oracle's to 1e-14)."""
+    own LAMBTEST starts from a 2:1 ellipsoid, far outside it).  The z
+    half-axis swings through one clean cycle (trough near step 1200, peak near
+    2450, trough near 3400); after it the damped mode gives way to wiggles of
+    about 0.1 node, where counting every local maximum above the mean (the
+    reference's mean_period) picks up noise and moves with the last bits of
+    the arithmetic.  So the period is the first cycle's, trough to trough,
+    in FP32 and FP64 storage: the two agree to 0.5 % and along the series to
+    1e-3 nodes, and the period is 1.3-1.6 times Lamb's with the reference's
+    viscous correction -- measured 1.45, the scheme's, with a width-4
+    interface on R = 20 and the phase-field relaxation (the FP64 step equals
+    the oracle's to 1e-14)."""
     n, R, sig, nu, W, eps = 128, 20.0, 0.03, 0.001, 4.0, 0.05
     c = n / 2
     x = np.arange(1, n + 1) - c
@@ -372,18 +379,31 @@ def test_lamb_oscillation_frequency():
     phi = 0.5 * (1 - np.tanh((r - R * (1 + eps * 0.5 * (3 * ct * ct - 1))) / (0.5 * W)))
     m = np.zeros((10, n, n, n))
     m[0] = phi * (2 * sig) / R / (1.0 / 3.0)  # the reference's Laplace pressure, rho_phi = 1
-    p = L.Params(lx=n, ly=n, lz=n, lattice=27, highorder=1, twocomponent=1, visc1=nu, visc2=nu, sigma=sig,
-                 width=W, tau_diff=0.1, printphi=1)
-    s = L.Solver(p)
-    s.set_fields(m, phi)
-    steps, dosc = [], []
-    for k in range(400):
-        rho, _, _ = s.get_print()
-        steps.append(k * 20)
-        dosc.append(ST.lamb_observables(rho)[2])
-        s.step(20)
-    s.close()
+    runs = {}
+    for storage in ("f32", "f64"):
+        p = L.Params(lx=n, ly=n, lz=n, lattice=27, highorder=1, twocomponent=1, visc1=nu, visc2=nu, sigma=sig,
+                     width=W, tau_diff=0.1, printphi=1, storage=storage)
+        s = L.Solver(p)
+        s.set_fields(m, phi)
+        steps, dosc = [], []
+        for k in range(181):
+            rho, _, _ = s.get_print()
+            steps.append(k * 20)
+            dosc.append(ST.lamb_observables(rho)[2])
+            s.step(20)
+        s.close()
+        runs[storage] = (np.array(steps, dtype=np.float64), np.array(dosc))
     T_th = 2 * np.pi / ST.lamb_theory_omega(sig, R, 1.0, 1.0, nu, nu)
-    T_num, npeaks = ST.mean_period(steps, dosc, 0.5 * T_th)
-    assert npeaks >= 3, (npeaks, dosc[::10])
-    assert 1.0 <= T_num / T_th < 1.4, (T_num, T_th)
+    ex = {k: ST.first_extrema(*v, 3) for k, v in runs.items()}
+    for k, e in ex.items():
+        assert [kind for _, _, kind in e] == ["min", "max", "min"], (k, e)
+    T = {k: e[2][0] - e[0][0] for k, e in ex.items()}
+    dev = float(np.max(np.abs(runs["f32"][1] - runs["f64"][1])))
+    print(f"lamb first cycle: period FP32 {T['f32']:.1f} FP64 {T['f64']:.1f} steps, "
+          f"{T['f64'] / T_th:.3f} x Lamb's {T_th:.1f}; max |FP32 - FP64| of the z half-axis {dev:.2e}")
+    assert abs(T["f32"] / T["f64"] - 1) < 0.005, T
+    assert dev < 1e-3, dev
+    assert 1.3 <= T["f64"] / T_th <= 1.6, (T, T_th)
+    # damped: the second trough is shallower than the first
+    e = ex["f64"]
+    assert e[2][1] > e[0][1], e

@@ -270,3 +270,18 @@ def test_printhalf_files_in_the_reference_layout(tmp_path):
     assert np.array_equal(v, np.moveaxis(vel, 0, -1).astype(np.float16).view(np.uint16))
     x = (tmp_path / "out_vel_000004.xdmf").read_text()
     assert 'NumberType="UInt" Precision="2" Dimensions="3 5 12 3"' in x
+
+
+def test_first_extrema_of_a_damped_oscillation():
+    """statistics.first_extrema: the first cycle of a damped cosine sampled
+    every 20 steps, followed by small wiggles that would add local maxima."""
+    from lbfast_b200 import statistics as ST
+    T, tau = 2200.0, 6000.0
+    t = np.arange(0, 8000, 20, dtype=np.float64)
+    d = 20.3 + 0.9 * np.exp(-t / tau) * np.cos(2 * np.pi * t / T) + 0.05 * np.sin(2 * np.pi * t / 230.0) * (t > 4000)
+    ex = ST.first_extrema(t, d, 3)
+    assert [k for _, _, k in ex] == ["min", "max", "min"]
+    # a damped cosine's extrema sit slightly before the undamped ones
+    assert abs(ex[0][0] - T / 2) < 40 and abs(ex[1][0] - T) < 40 and abs(ex[2][0] - 1.5 * T) < 40, ex
+    assert abs((ex[2][0] - ex[0][0]) - T) < 10, ex
+    assert ex[2][1] > ex[0][1]
