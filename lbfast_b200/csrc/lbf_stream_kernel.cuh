@@ -110,7 +110,7 @@ __device__ __forceinline__ void d1q3n2(T m0, T m1, T m2n, T& vm, T& v0, T& vp) {
 
 template <int LAT, bool TC, typename S, typename R, int TYV> constexpr size_t stream_smem_bytes() {
     constexpr int R1N = Tile<TYV>::R1N, R2N = Tile<TYV>::R2N, R3N = Tile<TYV>::R3N;
-    size_t b = sizeof(R) * size_t(27) * R1N;  // populations: 9 (cx, cy) groups x 3 cz
+    size_t b = sizeof(R) * size_t(24) * R1N;  // populations: 8 (cx, cy) groups x 3 cz (the centre stays in registers)
     if (TC)
         b += sizeof(R) * (size_t(PHI_SLOTS) * R3N + size_t(SXY_SLOTS) * R2N + size_t(GXY_SLOTS) * 2 * R2N +
                           size_t(TH_SLOTS) * 3 * R2N + size_t(GT_SLOTS) * 3 * R1N + size_t(H_SLOTS) * 3 * R1N);
@@ -135,9 +135,12 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     // post-collision populations of plane q, by (cx, cy) group g = 3 (cy+1) + (cx+1):
     // the output nodes that read one group of a node read all three cz of it
     using R2 = typename Vec2<R>::type;
-    R2* pops2 = reinterpret_cast<R2*>(smem_raw);                  // [9][R1N] (cz = -1, cz = 0)
-    R* pops1 = reinterpret_cast<R*>(pops2 + 9 * R1N);             // [9][R1N] (cz = +1)
-    R* phis = pops1 + 9 * R1N;                         // [PHI_SLOTS][R3N]     (TC)
+    // (the centre group (0, 0) of a node is read only by the node's own
+    // output, the thread that collided it: it stays in registers)
+    R2* pops2 = reinterpret_cast<R2*>(smem_raw);                  // [8][R1N] (cz = -1, cz = 0)
+    R* pops1 = reinterpret_cast<R*>(pops2 + 8 * R1N);             // [8][R1N] (cz = +1)
+    R* phis = pops1 + 8 * R1N;                         // [PHI_SLOTS][R3N]     (TC)
+    auto gslot = [](int g) { return g < 4 ? g : g - 1; };  // shared slot of group g != 4
     R* sxys = phis + (TC ? PHI_SLOTS * R3N : 0);       // [SXY_SLOTS][R2N]     (TC) S_x S_y phi
     R* gxys = sxys + (TC ? SXY_SLOTS * R2N : 0);       // [GXY_SLOTS][2][R2N]  (TC) D_x S_y phi, S_x D_y phi
     R* ths = gxys + (TC ? GXY_SLOTS * 2 * R2N : 0);    // [TH_SLOTS][3][R2N]   (TC) theta
@@ -513,6 +516,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             theta_plane(q + 2);
         }
 
+        R c4m = R(0), c40 = R(0), c4p = R(0);  // centre group of the interior node
         // unrolled: the interior node's copy of the collision reads the
         // prefetched registers in place (one shared copy of the loop body
         // costs moves and selects between the two sources: 6 % more
@@ -787,8 +791,8 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                             R2 v2;
                             v2.x = vm;
                             v2.y = v0;
-                            pops2[(3 * b + xg) * R1N + node] = v2;
-                            pops1[(3 * b + xg) * R1N + node] = vp;
+                            pops2[gslot(3 * b + xg) * R1N + node] = v2;
+                            pops1[gslot(3 * b + xg) * R1N + node] = vp;
                         }
                         ring_done = true;
                     } else {
@@ -835,8 +839,8 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                                 R2 v2;
                                 v2.x = vm;
                                 v2.y = v0;
-                                pops2[(3 * yg + a) * R1N + node] = v2;
-                                pops1[(3 * yg + a) * R1N + node] = vp;
+                                pops2[gslot(3 * yg + a) * R1N + node] = v2;
+                                pops1[gslot(3 * yg + a) * R1N + node] = vp;
                             }
                             ring_done = true;
                         } else {
@@ -886,8 +890,18 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
                 R2 v;
                 v.x = IN<LAT>(LINK(cx, cy, -1)) ? fpop[LINK(cx, cy, -1)] : R(0);
                 v.y = IN<LAT>(LINK(cx, cy, 0)) ? fpop[LINK(cx, cy, 0)] : R(0);
-                pops2[g * R1N + node] = v;
-                pops1[g * R1N + node] = IN<LAT>(LINK(cx, cy, 1)) ? fpop[LINK(cx, cy, 1)] : R(0);
+                const R vp = IN<LAT>(LINK(cx, cy, 1)) ? fpop[LINK(cx, cy, 1)] : R(0);
+                if (g == 4) {
+                    // the centre group: only the interior node's own output reads it
+                    if (k == 0) {
+                        c4m = v.x;
+                        c40 = v.y;
+                        c4p = vp;
+                    }
+                    continue;
+                }
+                pops2[gslot(g) * R1N + node] = v;
+                pops1[gslot(g) * R1N + node] = vp;
             }
 
             // ---- obstacle bounce-back: lb_cuda_boundary_module.f90:162-199 ----
@@ -933,10 +947,15 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
 #pragma unroll
             for (int xc = 0; xc < 3; ++xc) {
                 const int g = 3 * yc + xc;
+                if (g == 4) {
+                    gp[yc][xc] = PK<R>::mk(c4m, c40);
+                    gs[yc][xc] = c4p;
+                    continue;
+                }
                 const int src = (ty + 1 - (yc - 1)) * R1X + (tx + 1 - (xc - 1));
-                const R2 v = pops2[g * R1N + src];
+                const R2 v = pops2[gslot(g) * R1N + src];
                 gp[yc][xc] = PK<R>::mk(v.x, v.y);
-                gs[yc][xc] = pops1[g * R1N + src];
+                gs[yc][xc] = pops1[gslot(g) * R1N + src];
             }
         {
             using P = PK<R>;
