@@ -211,17 +211,6 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     const bool out_ok = (ox < nx) && (oy < ny);
     const int out_off = oy * nx + ox;
 
-    // neighbour x / y coordinates of the output node (bounce-back isfluid tests)
-    int nbx[3], nby[3];
-    bool nbx_ok[3], nby_ok[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        bool okx = true, oky = true;
-        nbx[d] = wrap_coord(ox + d - 1, nx, p.pbx, okx);
-        nby[d] = wrap_coord(oy + d - 1, ny, p.pby, oky);
-        nbx_ok[d] = okx;
-        nby_ok[d] = oky;
-    }
 
     // theta nodes (R2): slot n = t + k NTH of the first NTH threads; phi nodes
     // (R3): t, t + NT, t + 2 NT.  Slot n maps to the first TX columns of each
@@ -350,6 +339,23 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
     // theta = phi(1-phi) n on the theta region and g~ = n |g| on the collision
     // region of plane q (compute_norm_interface, lb_cuda_auxfields_module.f90:72-119)
     // from the partials of planes q-1..q+1
+    // Obstacles: isfluid of this thread's theta nodes in plane q (0 outside
+    // the box), loaded a plane before theta_plane uses it so the load's
+    // latency passes behind the pull phase; a load at the point of use
+    // stalled every theta warp at once (a box with obstacles stepped 33 %
+    // slower than without, with no solid node)
+    auto theta_isf = [&](int q, int8_t (&s)[KTH]) {
+        bool zk = true;
+        const int wz = zwrap(q, zk);
+#pragma unroll
+        for (int k = 0; k < KTH; ++k) {
+            const int n = t + k * NTH;
+            s[k] = (t < NTH && n < R2N && zk && r2_ok[k]) ? p.isf[wz * plane + r2_off[k]] : int8_t(0);
+        }
+    };
+    int8_t th_isf[KTH];
+#pragma unroll
+    for (int k = 0; k < KTH; ++k) th_isf[k] = 1;
     auto theta_plane = [&](int q) {
         bool zok = true;
         const int wz = zwrap(q, zok);
@@ -371,10 +377,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             r2_node(n, hx, hy);
             const int m = hy * R2X + hx;
             bool fluid = zok && r2_ok[k];
-            if (fluid && obs) {
-                const int s = p.isf[wz * plane + r2_off[k]];
-                fluid = (s == 1 || s == -1);
-            }
+            if (fluid && obs) fluid = (th_isf[k] == 1 || th_isf[k] == -1);
             R th0 = 0, th1 = 0, th2 = 0, gv0 = 0, gv1 = 0, gv2 = 0;
             if (fluid) {
                 const R gx = R(3) * (W1 * (g0[m] + g2[m]) + W0 * g1[m]);
@@ -484,15 +487,19 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         planar_plane(z0 - 3);
         planar_plane(z0 - 2);
         planar_plane(z0 - 1);
+        if (obs) theta_isf(z0 - 2, th_isf);
         theta_plane(z0 - 2);
         planar_plane(z0);
+        if (obs) theta_isf(z0 - 1, th_isf);
         theta_plane(z0 - 1);
         planar_plane(z0 + 1);
         __syncthreads();
         theta_partials(z0 - 2);
         theta_partials(z0 - 1);
         __syncthreads();
+        if (obs) theta_isf(z0, th_isf);
         theta_plane(z0);               // into the slot of theta(z0-2)
+        if (obs) theta_isf(z0 + 1, th_isf);  // for the loop's first theta plane
         load_phi_plane(z0 + 2, true);  // into the slot of phi(z0-3), no longer read
     }
     prefetch_a(z0 - 1);
@@ -907,6 +914,20 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
             // ---- obstacle bounce-back: lb_cuda_boundary_module.f90:162-199 ----
             if (interior && obs && isf == -1) {
                 const R om1 = R(1) - som;
+                // neighbour x / y coordinates of the output node, computed here:
+                // held in registers through the whole sweep they cost the
+                // obstacle step 4 registers at its limit of 128 and 10.7 % of
+                // its time on a box with obstacles
+                int nbx[3], nby[3];
+                bool nbx_ok[3], nby_ok[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    bool okx = true, oky = true;
+                    nbx[d] = wrap_coord(ox + d - 1, nx, p.pbx, okx);
+                    nby[d] = wrap_coord(oy + d - 1, ny, p.pby, oky);
+                    nbx_ok[d] = okx;
+                    nby_ok[d] = oky;
+                }
 #pragma unroll
                 for (int l = 1; l < 27; ++l) {
                     if (!IN<LAT>(l)) continue;
@@ -936,6 +957,7 @@ __device__ __forceinline__ void step_body(const StepParams<S, R>& p, const int b
         // the slot of phi(q-1) was last read in phase 1
         prefetch_a(q + 1);
         if constexpr (TC) load_phi_plane(q + 4, true);
+        if (TC && obs) theta_isf(q + 3, th_isf);  // for theta(q+3), next plane
 
         // the three cz populations of every (cx, cy) group from node x - c:
         // cz = -1, 0 as one pair (packed sums), cz = +1 alone
