@@ -61,10 +61,10 @@ RHO_R, RHO_B = 100.0, 1.0
 B_LUP = {"f32": 112, "f16": 76, "bf16": 76, "f64": 224}
 # DRAM bytes (read + write) of one step launch of the tuned kernel, measured
 # by ncu (dram__bytes_read.sum + dram__bytes_write.sum) at this workload
-NCU_TRAFFIC = {("f32", 256): 1853379072}
+NCU_TRAFFIC = {("f32", 256): 1882172928}
 # warp instructions of one step launch (ncu smsp__inst_executed.sum) at this
 # workload: the issue ceiling is 4 warp instructions per SM cycle
-NCU_WARP_INST = {("f32", 256): 698.75e6}
+NCU_WARP_INST = {("f32", 256): 707.22e6}
 
 
 CHANNEL = (512, 256, 256)  # the two-component channel with obstacles (lx, ly, lz)
@@ -609,7 +609,8 @@ def main():
     ap.add_argument("--workload", default="laplace", choices=["laplace", "channel"],
                     help="laplace: the droplet box (headline); channel: 512x256x256 with obstacles")
     ap.add_argument("--tile", type=int, default=0, help="kernel tile rows (8 or 16); 0: autotuned")
-    ap.add_argument("--zseg", type=int, default=0, help="planes per z segment; 0: autotuned / automatic")
+    ap.add_argument("--zseg", type=int, default=0,
+                    help="planes per z segment; negative: columns split at plane -zseg; 0: autotuned / automatic")
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-solves", type=int, default=40, help="solves of the serving measurement (0: skip)")

@@ -68,12 +68,14 @@ typedef struct lbf_params {
                                 applies it only with WETTABILITY and otherwise uses 90
                                 (lb_cuda_boundary_module.f90:264,275) */
     int printphi;            /* PRINTPHI: `rho` output holds phi */
-    int zseg;                /* planes per z segment of the kernel (one CTA per tile and segment); 0 = a
+    int zseg;                /* planes per z segment of the kernel (one CTA per tile and segment); < 0 =
+                                split columns: per column one CTA for planes [0, -zseg) and one for the
+                                rest (for boxes whose columns fill less than one wave of SMs); 0 = a
                                 persistent schedule: one CTA per resident slot, each advancing an equal
                                 contiguous share of the box's columns x planes */
     int tile_y;              /* rows of the kernel's 32-wide tile: 8 or 16 (FP64: 8 only).  0 = 16 rows (8 in
                                 FP64) and, when zseg = 0, the schedule autotuned at the first lbf_step: each
-                                candidate (persistent, z segments of several lengths) is timed on the box
+                                candidate (persistent, z segments of several lengths, split columns) is timed on the box
                                 itself, the fastest is kept and remembered for boxes of the same shape and
                                 class.  The schedule does not change the results; the tile height may in
                                 the last bit (separate compilations). */
@@ -151,8 +153,8 @@ int lbf_sync(lbf_handle* h);
 
 /* Number of steps done since lbf_set_fields. */
 int lbf_get_step(lbf_handle* h, long long* step);
-/* The kernel tile height and z segment (0: persistent schedule) in use, after
- * the autotuner if it ran. */
+/* The kernel tile height and z segment (0: persistent schedule, < 0: columns
+ * split at plane -zseg) in use, after the autotuner if it ran. */
 int lbf_get_tuning(lbf_handle* h, int* tile_y, int* zseg);
 
 /* State a next step starts from: moments (10 x N), phi (N) and the velocity

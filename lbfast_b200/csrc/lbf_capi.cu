@@ -110,6 +110,29 @@ int auto_zseg(int nx, int ny, int nz, int tile_y) {
     return zseg;
 }
 
+// Split planes for a box whose columns fill less than one wave of CTA slots:
+// L such that the heads [0, L) on ncols slots and the tails [L, nzr) on the
+// other slots (ceil(ncols / free) rounds of them) end together, for tails
+// that run s times slower per plane (their halo re-reads miss the L2 that
+// columns in step share) and a pipeline fill of 4 planes per segment; s from
+// 1 to 1.5.  Measured at 256^3 (128 columns, 148 SMs): whole columns 1.027 ms,
+// split at 229 0.924, at 233 0.940, at 220 1.039 -- the tails become the
+// longer part below the optimum, so the autotuner times several planes.
+std::vector<int> split_planes(int nx, int ny, int nzr, int tile_y, int storage) {
+    std::vector<int> out;
+    const long long cols = (long long)((nx + 31) / 32) * ((ny + tile_y - 1) / tile_y);
+    const long long slots = lbf::resident_slots((tile_y == 8 && storage != LBF_STORE_F64) ? 2 : 1);
+    if (cols >= slots || nzr < 16) return out;
+    constexpr double FILL = 4.0;
+    const double rounds = (double)((cols + (slots - cols) - 1) / (slots - cols));
+    for (int i = 0; i <= 10; ++i) {
+        const double s = 1.0 + 0.05 * i;
+        const int L = (int)std::lround((rounds * (nzr + FILL) * s - FILL) / (1.0 + rounds * s));
+        if (L >= 8 && L < nzr && std::find(out.begin(), out.end(), L) == out.end()) out.push_back(L);
+    }
+    return out;
+}
+
 // ---- autotuner of the schedule ----
 // The tile height is fixed per storage (default_tile): kernels of different
 // tile heights are different compilations whose floating-point contractions
@@ -152,8 +175,8 @@ int autotune(lbf_handle* h) {
     std::vector<std::pair<int, int>> cand;
     for (int ty : {h->tile_y}) {
         std::vector<int> zs;
-        if (h->p.zseg > 0) {
-            zs.push_back(std::min(h->p.zseg, h->nz));
+        if (h->p.zseg != 0) {
+            zs.push_back(h->zseg);
         } else {
             // the persistent schedule (0), and fixed segments: about four waves,
             // half and twice that, and whole columns.  Segments keep the CTAs
@@ -161,7 +184,10 @@ int autotune(lbf_handle* h) {
             // halo re-reads hit in L2; the persistent schedule balances the SMs
             // exactly but staggers neighbours in z.
             const int za = auto_zseg(h->nx, h->ny, h->nz, ty), lo = std::min(h->nz, 8);
-            for (int z : {0, za, std::max(lo, za / 2), std::min(h->nz, 2 * za), h->nz})
+            std::vector<int> all = {0, za, std::max(lo, za / 2), std::min(h->nz, 2 * za), h->nz};
+            // split columns (negative: the split plane)
+            for (int L : split_planes(h->nx, h->ny, h->slab ? h->nzs : h->nz, ty, h->storage)) all.push_back(-L);
+            for (int z : all)
                 if (std::find(zs.begin(), zs.end(), z) == zs.end()) zs.push_back(z);
         }
         for (int z : zs) cand.emplace_back(ty, z);
@@ -373,7 +399,8 @@ int lbf_create(const lbf_params* p, lbf_handle** out) {
         delete h;
         return fail(LBF_E_UNSUPPORTED, "no kernel for this configuration");
     }
-    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : 0;  // 0: persistent schedule
+    // > 0: z segments; < 0: columns split at plane -zseg; 0: persistent schedule
+    h->zseg = p->zseg > 0 ? std::min(p->zseg, p->lz) : (p->zseg < 0 ? std::max(p->zseg, -p->lz) : 0);
     bool ok = true;
     for (int b = 0; b < 2 && ok; ++b) {
         // 16-bit storage: Pi - u u (6 fields) in 16 bits, P, u, v, w in FP32 (pres)

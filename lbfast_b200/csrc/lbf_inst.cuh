@@ -57,6 +57,12 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t st) {
     make_params(a, p);
     const int nzr = a.zhi - a.zlo;
     if (nzr <= 0) return cudaSuccess;
+    if (a.zseg < 0) {
+        // split columns: a head and a tail segment per column
+        const long long ncols = (long long)((a.nx + TX - 1) / TX) * ((a.ny + TYV - 1) / TYV);
+        stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<(unsigned)(2 * ncols), TX * TYV, smem, st>>>(p);
+        return cudaGetLastError();
+    }
     if (a.zseg > 0) {
         dim3 grid((a.nx + TX - 1) / TX, (a.ny + TYV - 1) / TYV, (nzr + a.zseg - 1) / a.zseg);
         stream_kernel<LAT, HO, TC, S, R, TYV, REP, OBS><<<grid, TX * TYV, smem, st>>>(p);

@@ -1085,7 +1085,11 @@ __device__ __forceinline__ void run_share(const int nx, const int nzr, const int
 }
 
 // Single box.  zseg > 0: one CTA per (tile x, tile y, z segment of zseg
-// planes).  zseg = 0: persistent schedule -- the box's columns x planes are
+// planes).  zseg < 0: split columns -- CTA i < ncols advances planes [0, L)
+// of column i and CTA ncols + i planes [L, nzr), L = -zseg: when the columns
+// fill less than one wave of CTA slots, the long segments run in step on
+// ncols SMs (their halo re-reads hit in L2) while the other SMs work through
+// the short tails.  zseg = 0: persistent schedule -- the box's columns x planes are
 // cut into gridDim.x equal contiguous shares (a share may end inside one
 // column and continue at the bottom of the next), so every CTA does the same
 // work and pays the pipeline fill of a segment start only once or twice.
@@ -1097,7 +1101,14 @@ template <int LAT, bool HO, bool TC, typename S, typename R, int TYV, bool REP =
 __global__ void __launch_bounds__(TX * TYV, step_min_blocks<R, TYV>()) stream_kernel(const StepParams<S, R> p) {
     long long s0, s1;
     const int nzr = p.zhi - p.zlo;
-    if (p.zseg > 0) {
+    if (p.zseg < 0) {
+        const int L = min(-p.zseg, nzr);
+        const long long ncols = (long long)((p.nx + TX - 1) / TX) * ((p.ny + TYV - 1) / TYV);
+        const bool head = blockIdx.x < ncols;
+        const long long col = head ? blockIdx.x : blockIdx.x - ncols;
+        s0 = col * nzr + (head ? 0 : L);
+        s1 = col * nzr + (head ? L : nzr);
+    } else if (p.zseg > 0) {
         const long long col = (long long)blockIdx.y * ((p.nx + TX - 1) / TX) + blockIdx.x;
         const int z0 = blockIdx.z * p.zseg;
         s0 = col * nzr + z0;

@@ -156,13 +156,14 @@ def _equal(a, b):
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_schedule_does_not_change_results(name, storage):
     """One kernel gives the same bits for every z segmentation, the persistent
-    schedule and the autotuned choice: each node's arithmetic does not depend
-    on the work decomposition.  Tiles of 8 rows are a separate compilation
+    schedule, columns split into a head and a tail segment, and the autotuned
+    choice: each node's arithmetic does not depend on the work decomposition.  Tiles of 8 rows are a separate compilation
     (its floating-point contractions may differ): equal within rounding."""
     p, isf, _, _ = make_case(name, storage)
     fl = np.abs(isf) == 1
     ref = _fields_with(name, storage, 9, tile_y=16, zseg=3)
-    for over in ({"tile_y": 16, "zseg": 0}, {"tile_y": 16, "zseg": 5}, {"tile_y": 0, "zseg": 0}):
+    for over in ({"tile_y": 16, "zseg": 0}, {"tile_y": 16, "zseg": 5}, {"tile_y": 16, "zseg": -5},
+                 {"tile_y": 16, "zseg": -1000}, {"tile_y": 0, "zseg": 0}):
         assert _equal(_fields_with(name, storage, 9, **over), ref), over
     m8, p8, _ = _fields_with(name, storage, 9, tile_y=8, zseg=0)
     bar = 1e-6 if storage == "f32" else 1e-3
