@@ -17,7 +17,9 @@
 //           2-node ring) and of theta (tile + 1-node ring)
 //   theta = phi(1-phi) n on the tile + 2-node ring and g~ = n|grad phi| on
 //           the tile + 1-node ring
-//   post-collision populations of plane q on the tile + 1-node ring.
+//   post-collision populations of plane q on the tile + 1-node ring (the
+//           centre group of a node, read only by its own output, stays in
+//           the registers of the thread that collided it).
 // Each output node then pulls f*_l(x - c_l) from shared memory: the nine
 // (cx,cy) populations of each cz slice of plane q go to output plane q+cz,
 // accumulated in registers; plane q-1 is complete after plane q and is

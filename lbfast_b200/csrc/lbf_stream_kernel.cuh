@@ -1,14 +1,17 @@
 // lbf_stream_kernel.cuh -- body of the fused step kernel (see lbf_stream.cuh).
 //
 // Per z plane q a CTA runs two barrier phases:
-//   phase 1  theta(q+2) on the theta region, and the moments prologue +
-//            collision of plane q on the collision region (populations to
-//            shared memory).  The two sets of work are independent, so one
-//            barrier covers both, and the halo-ring collisions are placed on
-//            the warps with the least theta work.
+//   phase 1  the in-plane partials of phi(q+3) and theta(q+2) on the theta
+//            region, and the moments prologue + collision of plane q on the
+//            collision region (populations to shared memory).  The two sets
+//            of work are independent, so one barrier covers both, and the
+//            halo-ring collisions are placed on the warps with no theta work.
+//            Before the barrier each thread issues the loads of its interior
+//            node's fields of plane q+1.
 //   phase 2  an asynchronous copy (cp.async) of phi(q+4) into its ring
-//            slot; then every output node pulls the populations of plane q
-//            and plane q-1 is written.  The copy completes behind this phase.
+//            slot; the theta partials of plane q+2; then every output node
+//            pulls the populations of plane q and plane q-1 is written.  The
+//            copy completes behind this phase.
 #pragma once
 #include "lbf_stream.cuh"
 
